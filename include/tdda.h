@@ -1,0 +1,171 @@
+/*
+ * libtdda — C ABI of the B200-native DDA forward/adjoint solve.
+ *
+ * Each entry point replaces one method of Topo-DDA's pybind11 `DDAModel`
+ * (python_bindings/PythonBindings.cpp:16-70); the reference file:line it
+ * stands in for is given beside it.  All arrays are plain host pointers unless
+ * the name ends in `_device`; complex arrays are interleaved (re, im) doubles
+ * in the reference's dipole order: element 3*i + c is component c of dipole i.
+ * Every call returns a tdda_status; tdda_last_error() gives the message of the
+ * last failure on the calling thread.  A model is not re-entrant: calls on one
+ * model must not overlap.
+ */
+#ifndef TDDA_H_
+#define TDDA_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    TDDA_OK = 0,
+    TDDA_ERR_BAD_ARG = 1,       /* reference: `throw 1` -> RuntimeError */
+    TDDA_ERR_OOM = 2,
+    TDDA_ERR_NOT_CONVERGED = 3, /* reported in tdda_solve_info, not returned by solves */
+    TDDA_ERR_BREAKDOWN = 4,
+    TDDA_ERR_CUDA = 5,
+    TDDA_ERR_TIMEOUT = 6,
+    TDDA_ERR_UNSUPPORTED = 7,
+    TDDA_ERR_STATE = 8
+} tdda_status;
+
+typedef enum {
+    TDDA_SOLVE_RUNNING = 0,
+    TDDA_SOLVE_CONVERGED = 1,   /* ||r||/||E|| <= tol (recursive residual) */
+    TDDA_SOLVE_MAXITER = 2,     /* reference prints "does not converge" */
+    TDDA_SOLVE_BREAKDOWN = 3,   /* r0 . rl == 0 (src/DDAModel.cpp:952-970) */
+    TDDA_SOLVE_NONFINITE = 4,   /* residual became NaN/Inf */
+    TDDA_SOLVE_ZERO_RHS = 5     /* ||E|| == 0: solution is 0 */
+} tdda_solve_status;
+
+typedef enum { TDDA_PREC_C128 = 0, TDDA_PREC_MIXED = 1 } tdda_precision;
+
+typedef struct tdda_model tdda_model;
+
+/* Constructor arguments of DDAModel (python_bindings/PythonBindings.cpp:19-46),
+ * minus the arrays, which tdda_model_create takes separately. */
+typedef struct {
+    double beta_min, beta_max, ita;   /* filter: accepted, unused (disabled on every Python path) */
+    const char *beta_type;
+    int use_filter;                   /* must be 0: the legacy filter is not on this path */
+    const char *symmetry_type;        /* "None" or "4fold" (src/DDAModel.cpp:163-173) */
+    double symmetry_axis[2];
+    int is_periodic;
+    const char *objective_name;       /* IntegratedE (the reference factory always builds it) */
+    const double *obj_para;
+    int n_obj_para;
+    int num_x, num_y, num_z, num_total;
+    double n_K[3];
+    double E0;
+    double n_E0[3];
+    double lam;
+    double material[4];               /* (re, im) of material[0], material[1] */
+    double nback;
+    int MAXm, MAXn;
+    double Lm, Ln;                    /* periods in units of d */
+    const char *matrix_method;        /* "FCD" or "LDR" */
+    double d;
+    double integral_delta;
+    int verbose;
+    int precision;                    /* tdda_precision */
+} tdda_params;
+
+typedef struct {
+    int iterations;      /* reference ITERATION */
+    double error;        /* reference Error: ||r||/||E|| */
+    int status;          /* tdda_solve_status */
+    int refinements;     /* outer complex128 refinement steps (mixed precision) */
+    int inner_iterations;/* total complex64 BiCGSTAB iterations (mixed precision) */
+    double true_error;   /* ||E - A P|| / ||E|| recomputed in complex128 (mixed precision) */
+} tdda_solve_info;
+
+typedef struct {
+    int N, NFpara;
+    int nx, ny, nz;
+    int Lx, Ly, Lz;
+    double K;
+    double material[4];  /* after the nback rescale (src/AProductCore.cpp:25-33) */
+    long long device_bytes;
+    double lattice_ms, tensor_fft_ms;
+} tdda_model_info;
+
+const char *tdda_status_string(tdda_status s);
+const char *tdda_last_error(void);
+int tdda_abi_version(void);
+
+/* DDAModel::DDAModel (src/DDAModel.cpp:79-333; binding PythonBindings.cpp:19-59):
+ * geometry int32[3N], input_dielectrics double[3N], si/ci double[ntab]. */
+tdda_status tdda_model_create(const tdda_params *p, const int32_t *geometry,
+                              const double *input_dielectrics, const double *si,
+                              const double *ci, int64_t ntab, tdda_model **out);
+/* DDAModel::~DDAModel (src/DDAModel.cpp:335-338) */
+void tdda_model_destroy(tdda_model *m);
+tdda_status tdda_model_get_info(const tdda_model *m, tdda_model_info *info);
+
+/* DDAModel::solveElectricField (src/DDAModel.cpp:874-885; binding :64).
+ * P0: complex[3N] or NULL for zeros. */
+tdda_status tdda_solve_electric_field(tdda_model *m, const double *P0, int max_iter, double tol,
+                                      tdda_solve_info *info);
+/* DDAModel::calculateObjective (src/DDAModel.cpp:870-872; binding :61) */
+tdda_status tdda_calculate_objective(tdda_model *m, double *out);
+/* DDAModel::calculateGradients (src/DDAModel.cpp:398-469; binding :62): the
+ * reference's one-sided finite-difference partials + adjoint solve.  grad: double[NFpara]. */
+tdda_status tdda_calculate_gradients(tdda_model *m, double epsilon_partial, double original_obj,
+                                     int max_iter, double tol, double *grad, int64_t n);
+/* DDAModel::UpdateParameters (src/DDAModel.cpp:747-772; binding :66) */
+tdda_status tdda_set_parameters(tdda_model *m, const double *values, int64_t n);
+/* DDAModel::get_parameter_copy (src/DDAModel.cpp:1341-1343; binding :67) */
+tdda_status tdda_get_parameters(const tdda_model *m, double *out, int64_t n);
+/* DDAModel::get_dielectrics_copy (src/DDAModel.cpp:1346-1348; binding :68): double[3N] */
+tdda_status tdda_get_dielectrics(const tdda_model *m, double *out, int64_t n);
+/* DDAModel::get_EResult (src/DDAModel.cpp:1254-1256; binding :69): complex[3N] */
+tdda_status tdda_get_electric_field(const tdda_model *m, double *out, int64_t n);
+/* DDAModel::get_P (src/DDAModel.cpp:1273-1275): complex[3N] */
+tdda_status tdda_get_polarization(const tdda_model *m, double *out, int64_t n);
+
+/* DDAModel::Aproductwithalb (src/DDAModel.cpp:1194-1203) when with_al != 0,
+ * AProductCore::Aproduct (src/AProductCore.cpp:461-515) otherwise.
+ * x, y: complex[3N] host arrays. */
+tdda_status tdda_matvec(tdda_model *m, const double *x, double *y, int with_al);
+
+/* Device-resident forms (pointers from cudaMalloc / torch; stream may be NULL).
+ * Batched solve of (A + diag(1/alpha)) X_k = B_k for k < nrhs, complex[nrhs][3N]
+ * in dipole order; B == NULL uses the model's incident field for every k.
+ * Same BiCGSTAB as tdda_solve_electric_field (src/DDAModel.cpp:899-1009). */
+tdda_status tdda_solve_batch_device(tdda_model *m, const void *B_dev, void *X_dev, int nrhs,
+                                    int x0_zero, int max_iter, double tol, void *stream,
+                                    tdda_solve_info *infos);
+tdda_status tdda_matvec_device(tdda_model *m, const void *x_dev, void *y_dev, int nrhs,
+                               int with_al, void *stream);
+
+/* --- extensions (no single reference counterpart) --------------------------
+ * Per-dipole design densities rho[N] in [0, 1] (a 3-D design instead of the
+ * reference's z-extruded columns, DDAModel::UpdateParameters
+ * src/DDAModel.cpp:747-772); sets 1/alpha per dipole. */
+tdda_status tdda_set_densities(tdda_model *m, const double *rho, int64_t n);
+/* Exact adjoint gradient of the IntegratedE objective with respect to every
+ * dipole's density (the analytic form of calculateGradients,
+ * src/DDAModel.cpp:398-578): uses the polarisation of the last solve,
+ * runs one adjoint solve, grad: double[N]. */
+tdda_status tdda_gradient_densities(tdda_model *m, int max_iter, double tol, double *grad, int64_t n,
+                                    tdda_solve_info *info);
+/* Timing of the fused operator on the model's stream (CUDA events):
+ * ms_matvec = mean time of one A.x (three kernels) for nrhs right-hand
+ * sides, ms_pass[3] = mean time of each pass.  precision: 0 complex128,
+ * 1 complex64 (mixed-precision models only). */
+tdda_status tdda_profile_matvec(tdda_model *m, int precision, int nrhs, int iters, double *ms_matvec,
+                                double *ms_pass);
+/* Kernels launched by this library since load (all models). */
+long long tdda_kernel_launches(void);
+/* Solve precision of later solves: TDDA_PREC_C128, or TDDA_PREC_MIXED when
+ * the model was created mixed (its complex64 operator exists). */
+tdda_status tdda_set_precision(tdda_model *m, int precision);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TDDA_H_ */

@@ -1,0 +1,30 @@
+// Interaction-tensor assembly (lattice sums + FFT) on the device.
+#pragma once
+
+#include "tdda_common.cuh"
+#include "../../include/tdda.h"
+
+namespace tdda {
+
+struct LatticeParams {
+    int nx, ny, nz;       // box (octant extents)
+    int Lx, Ly, Lz;       // padded grid
+    double d;             // dipole spacing
+    double K;             // 2 pi nback / lam
+    double Kf;            // pi / d
+    double Lm, Ln;        // periods as lengths (d included)
+    int MAXm, MAXn;
+    int method;           // 0 FCD, 1 LDR
+    double gamma;         // damping exp(-(gamma K r)^4), 0.01 in the reference
+    double delta;         // SiCi table spacing
+    const double2 *sc;    // device (si, ci) pairs
+    long ntab;
+};
+
+// Lattice sums -> padded grid -> FP64 FFT -> folded spectral tensor
+// [hy][hx][hz][6] (scaled by 1/(Lx Ly Lz)); ahat32 optional complex64 copy.
+tdda_status build_tensor(const LatticeParams &P, const double *si, const double *ci, long ntab,
+                         double2 *ahat, float2 *ahat32, cudaStream_t s, double *lattice_ms,
+                         double *fft_ms);
+
+}  // namespace tdda

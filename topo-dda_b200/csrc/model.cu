@@ -1,0 +1,1094 @@
+// The DDAModel state machine behind the C ABI (include/tdda.h).
+//
+// Reference: src/DDAModel.cpp (constructor :79-333, parameter map :163-247,
+// polarisability :319-328/:1122-1151, solve :874-885, E_int :1185-1192,
+// objective via src/ObjDDAModel.cpp:103-218, gradient :398-578).  Host code
+// keeps the O(N) bookkeeping (parameter map, segmented sums over the
+// parameter -> dipole lists); everything on the solve path runs on the device.
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <complex>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "lattice.cuh"
+#include "operator.cuh"
+
+namespace tdda {
+
+static std::atomic<long long> g_launches{0};
+void count_launches(long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+long long launches_total() { return g_launches.load(std::memory_order_relaxed); }
+
+static thread_local std::string g_err;
+void set_error(const std::string &msg) { g_err = msg; }
+const char *get_error() { return g_err.c_str(); }
+
+// ----------------------------------------------------------------------------
+// device helpers of the model layer
+// ----------------------------------------------------------------------------
+// polarisability of the lattice dispersion relation, 1/alpha
+// (src/Tools.cpp:353-366; interpolation src/DDAModel.cpp:319-328)
+struct AlphaParams {
+    double lam, K, d;
+    double2 m0, m1;   // rescaled materials
+    double S;         // sum_c (n_E0,c n_K,c)^2
+};
+
+__host__ __device__ inline double2 cmul_d(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+__host__ __device__ inline double2 diel_of(double rho, const AlphaParams &A) {
+    // labelfloor = floor(rho), labelnext = floor+1 unless floor >= 1
+    double lf = floor(rho);
+    double2 mf = lf >= 1.0 ? A.m1 : A.m0;
+    double2 mn = (lf >= 1.0 || lf + 1.0 >= 1.0) ? A.m1 : A.m0;
+    double w = rho - lf;
+    return make_double2(mf.x + w * (mn.x - mf.x), mf.y + w * (mn.y - mf.y));
+}
+
+__host__ __device__ inline double2 inv_alpha(double2 eps, const AlphaParams &A) {
+    // same operation order as Get_Alpha (src/Tools.cpp:353-366)
+    const double b1 = -1.891531, b2 = 0.1648469, b3 = -1.7700004;
+    const double d3 = A.d * A.d * A.d;
+    const double pre = 3.0 * d3 / (4.0 * M_PI);
+    double2 num = make_double2(pre * (eps.x - 1.0), pre * eps.y);
+    double2 a1 = cdiv(num, make_double2(eps.x + 2.0, eps.y));
+    const double kd = A.K * A.d;
+    const double kd2 = kd * kd;
+    double2 rad = make_double2(0.0, (2.0 / 3.0) * (kd * kd * kd));
+    // (b1 + eps b2 + eps b3 S) (Kd)^2 - rad
+    double2 poly = make_double2(b1 + eps.x * b2 + (eps.x * b3) * A.S, eps.y * b2 + (eps.y * b3) * A.S);
+    double2 t = make_double2(poly.x * kd2 - rad.x, poly.y * kd2 - rad.y);
+    double2 a1d = make_double2(a1.x / d3, a1.y / d3);
+    double2 res = cmul_d(a1d, t);
+    res.x = 1.0 + res.x;
+    double2 alpha = cdiv(a1, res);
+    return cdiv(make_double2(1.0, 0.0), alpha);
+}
+
+__global__ void k_alpha(long long nbox, const double *__restrict__ rho, const unsigned char *__restrict__ mask,
+                        AlphaParams A, double2 *__restrict__ al, float2 *__restrict__ al32,
+                        double2 *__restrict__ diel) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nbox; i += (long long)gridDim.x * blockDim.x) {
+        double2 a, e;
+        if (mask != nullptr && mask[i] == 0) {
+            a = make_double2(1.0, 0.0);
+            e = make_double2(1.0, 0.0);
+        } else {
+            e = diel_of(rho[i], A);
+            a = inv_alpha(e, A);
+        }
+        al[i] = a;
+        diel[i] = e;
+        if (al32 != nullptr) al32[i] = make_float2((float)a.x, (float)a.y);
+    }
+}
+
+// dipole order (3*i + c, interleaved complex) <-> internal [rhs][c][cell]
+__global__ void k_scatter(int nrhs, long long N, long long nbox, const long long *__restrict__ cell_of,
+                          const double2 *__restrict__ ext, double2 *__restrict__ in) {
+    long long tot = (long long)nrhs * N * 3;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < tot; e += (long long)gridDim.x * blockDim.x) {
+        long long k = e / (3 * N), rem = e - k * 3 * N;
+        long long i = rem / 3;
+        int c = (int)(rem - i * 3);
+        in[((size_t)k * 3 + c) * nbox + cell_of[i]] = ext[e];
+    }
+}
+
+__global__ void k_gather(int nrhs, long long N, long long nbox, const long long *__restrict__ cell_of,
+                         const double2 *__restrict__ in, double2 *__restrict__ ext) {
+    long long tot = (long long)nrhs * N * 3;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < tot; e += (long long)gridDim.x * blockDim.x) {
+        long long k = e / (3 * N), rem = e - k * 3 * N;
+        long long i = rem / 3;
+        int c = (int)(rem - i * 3);
+        ext[e] = in[((size_t)k * 3 + c) * nbox + cell_of[i]];
+    }
+}
+
+// EResult = E_int = al P / ((2 + eps) / 3)   (src/DDAModel.cpp:1185-1192)
+__global__ void k_eresult(long long nbox, const double2 *__restrict__ P, const double2 *__restrict__ al,
+                          const double2 *__restrict__ diel, double2 *__restrict__ Eres) {
+    long long tot = 3 * nbox;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < tot; e += (long long)gridDim.x * blockDim.x) {
+        long long cell = e % nbox;
+        double2 lf = make_double2((2.0 + diel[cell].x) / 3.0, diel[cell].y / 3.0);
+        Eres[e] = cdiv(cmul_d(al[cell], P[e]), lf);
+    }
+}
+
+__device__ __forceinline__ double powabs(double2 z, int q) {
+    double a = hypot(z.x, z.y);
+    if (q == 2) return a * a;
+    return pow(a, (double)q);
+}
+
+// per-block partial sums of sum_c |al P_c|^q over dipole cells
+__global__ void k_objective(long long nbox, const double2 *__restrict__ P, const double2 *__restrict__ al,
+                            const unsigned char *__restrict__ mask, int q, double *__restrict__ part) {
+    double s = 0.0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nbox; i += (long long)gridDim.x * blockDim.x) {
+        if (mask != nullptr && mask[i] == 0) continue;
+        double2 a = al[i];
+        for (int c = 0; c < 3; ++c) s += powabs(cmul_d(a, P[(size_t)c * nbox + i]), q);
+    }
+    __shared__ double red[32];
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        s = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+        for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+        if (threadIdx.x == 0) part[blockIdx.x] = s;
+    }
+}
+
+// Finite-difference partials of the reference gradient
+// (devx_and_Adevxp src/DDAModel.cpp:471-536, devp :538-578), per dipole cell:
+//   dS[cell]     = sum_c |al' P_c|^q - |al P_c|^q  with al' = al(rho + sign eps)
+//   change[cell] = (al' - al) / (sign eps)
+//   devp[c][cell]= (log(S - base + c_re) - J0)/eps + (log(S - base + c_im) - J0)/(i eps)
+struct GradFD {
+    AlphaParams A;
+    double eps, J0, S;
+    int q;
+};
+
+__global__ void k_grad_fd(long long nbox, const double *__restrict__ rho, const unsigned char *__restrict__ mask,
+                          const double2 *__restrict__ P, const double2 *__restrict__ al, GradFD G,
+                          double *__restrict__ dS, double2 *__restrict__ change, double2 *__restrict__ devp) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nbox; i += (long long)gridDim.x * blockDim.x) {
+        if (mask != nullptr && mask[i] == 0) {
+            dS[i] = 0.0;
+            change[i] = make_double2(0.0, 0.0);
+            for (int c = 0; c < 3; ++c) devp[(size_t)c * nbox + i] = make_double2(0.0, 0.0);
+            continue;
+        }
+        const double r0 = rho[i];
+        const double sgn = r0 >= G.eps ? -1.0 : 1.0;
+        const double2 a = al[i];
+        const double2 an = inv_alpha(diel_of(r0 + sgn * G.eps, G.A), G.A);
+        double old = 0.0, nw = 0.0;
+        double2 Pc[3];
+        double cold[3];
+        for (int c = 0; c < 3; ++c) {
+            Pc[c] = P[(size_t)c * nbox + i];
+            cold[c] = powabs(cmul_d(a, Pc[c]), G.q);
+            old += cold[c];
+            nw += powabs(cmul_d(an, Pc[c]), G.q);
+        }
+        dS[i] = nw - old;
+        const double se = sgn * G.eps;
+        change[i] = make_double2((an.x - a.x) / se, (an.y - a.y) / se);
+        const double base = G.S - old;
+        for (int c = 0; c < 3; ++c) {
+            double cre = old - cold[c] + powabs(cmul_d(a, make_double2(Pc[c].x + G.eps, Pc[c].y)), G.q);
+            double cim = old - cold[c] + powabs(cmul_d(a, make_double2(Pc[c].x, Pc[c].y + G.eps)), G.q);
+            double fre = (log(base + cre) - G.J0) / G.eps;
+            double fim = (log(base + cim) - G.J0) / G.eps;
+            // fre + fim / (i) = fre - i fim
+            devp[(size_t)c * nbox + i] = make_double2(fre, -fim);
+        }
+    }
+}
+
+// prod[cell] = change[cell] * sum_c lambda_c P_c  (non-conjugated, src/DDAModel.cpp:445-455)
+__global__ void k_grad_mult(long long nbox, const double2 *__restrict__ lam, const double2 *__restrict__ P,
+                            const double2 *__restrict__ change, double2 *__restrict__ prod) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nbox; i += (long long)gridDim.x * blockDim.x) {
+        double2 s = make_double2(0.0, 0.0);
+        for (int c = 0; c < 3; ++c) {
+            double2 v = cmul_d(lam[(size_t)c * nbox + i], P[(size_t)c * nbox + i]);
+            s.x += v.x;
+            s.y += v.y;
+        }
+        prod[i] = cmul_d(s, change[i]);
+    }
+}
+
+// R32[k] = R[k] * scale[k]   (scale 0 parks a finished right-hand side)
+__global__ void k_to32_batch(long long n, int nrhs, const double2 *__restrict__ a, const double *__restrict__ scale,
+                             float2 *__restrict__ b) {
+    long long tot = n * nrhs;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < tot; i += (long long)gridDim.x * blockDim.x) {
+        double s = scale[i / n];
+        b[i] = make_float2((float)(a[i].x * s), (float)(a[i].y * s));
+    }
+}
+
+// X[k] += w[k] * D32[k]
+__global__ void k_axpy32_batch(long long n, int nrhs, const double *__restrict__ w, const float2 *__restrict__ d,
+                               double2 *__restrict__ x) {
+    long long tot = n * nrhs;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < tot; i += (long long)gridDim.x * blockDim.x) {
+        double s = w[i / n];
+        x[i].x += s * (double)d[i].x;
+        x[i].y += s * (double)d[i].y;
+    }
+}
+
+// d(1/alpha)/d rho: (-3 / (c (eps - 1)^2) + (b2 + b3 S) K^2 / d) (m1 - m0),
+// c = 3 d^3 / (4 pi) -- the closed-form derivative of Get_Alpha's inverse.
+__host__ __device__ inline double2 dal_drho(double2 eps, const AlphaParams &A) {
+    const double b2 = 0.1648469, b3 = -1.7700004;
+    const double c = 3.0 * A.d * A.d * A.d / (4.0 * M_PI);
+    double2 em1 = make_double2(eps.x - 1.0, eps.y);
+    double2 sq = cmul_d(em1, em1);
+    double2 t = cdiv(make_double2(-3.0 / c, 0.0), sq);
+    t.x += (b2 + b3 * A.S) * A.K * A.K / A.d;
+    return cmul_d(t, make_double2(A.m1.x - A.m0.x, A.m1.y - A.m0.y));
+}
+
+// adjoint right-hand side dJ/dx - i dJ/dy of J = log S, S = sum |al P|^q:
+// q |al|^q |P|^(q-2) conj(P) / S
+__global__ void k_adjoint_rhs(long long nbox, const double2 *__restrict__ P, const double2 *__restrict__ al,
+                              const unsigned char *__restrict__ mask, int q, double S, double2 *__restrict__ rhs) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nbox; i += (long long)gridDim.x * blockDim.x) {
+        const bool on = mask == nullptr || mask[i] != 0;
+        const double2 a = al[i];
+        const double aq = pow(hypot(a.x, a.y), (double)q);
+        for (int c = 0; c < 3; ++c) {
+            double2 p = P[(size_t)c * nbox + i];
+            double w = 0.0;
+            if (on) {
+                double ap = hypot(p.x, p.y);
+                w = q == 2 ? 2.0 * aq / S : (ap > 0 ? q * aq * pow(ap, (double)(q - 2)) / S : 0.0);
+            }
+            rhs[(size_t)c * nbox + i] = make_double2(w * p.x, -w * p.y);
+        }
+    }
+}
+
+// grad = explicit - Re(sum_c lambda_c al' P_c), explicit = sum_c q |al|^(q-2) |P_c|^q Re(conj(al) al') / S
+__global__ void k_grad_analytic(long long nbox, const double *__restrict__ rho, const unsigned char *__restrict__ mask,
+                                const double2 *__restrict__ P, const double2 *__restrict__ al,
+                                const double2 *__restrict__ diel, const double2 *__restrict__ lam, AlphaParams A,
+                                int q, double S, double *__restrict__ grad) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nbox; i += (long long)gridDim.x * blockDim.x) {
+        if (mask != nullptr && mask[i] == 0) { grad[i] = 0.0; continue; }
+        const double2 a = al[i];
+        const double2 da = dal_drho(diel[i], A);
+        const double ra = a.x * da.x + a.y * da.y;  // Re(conj(a) a')
+        const double am = hypot(a.x, a.y);
+        double ex = 0.0, im = 0.0;
+        for (int c = 0; c < 3; ++c) {
+            double2 p = P[(size_t)c * nbox + i];
+            double ap = hypot(p.x, p.y);
+            ex += (q == 2 ? 2.0 * ap * ap : q * pow(am, (double)(q - 2)) * pow(ap, (double)q)) * ra;
+            double2 v = cmul_d(lam[(size_t)c * nbox + i], cmul_d(da, p));
+            im += v.x;
+        }
+        grad[i] = ex / S - im;
+    }
+}
+
+static unsigned grid_for(long long n, int bs = 256, unsigned cap = 148 * 16) {
+    long long g = (n + bs - 1) / bs;
+    if (g < 1) g = 1;
+    if (g > cap) g = cap;
+    return (unsigned)g;
+}
+
+}  // namespace tdda
+
+using namespace tdda;
+
+// ----------------------------------------------------------------------------
+// the model
+// ----------------------------------------------------------------------------
+struct tdda_model {
+    // constructor arguments
+    int Nx = 0, Ny = 0, Nz = 0, N = 0;
+    double d = 0, lam = 0, nback = 1, K = 0, E0 = 1;
+    double nK[3]{}, nE0[3]{};
+    double2 mat[2]{};
+    int MAXm = 0, MAXn = 0;
+    double Lm = 0, Ln = 0;  // lengths (d included)
+    int method = 0;
+    double delta = 0.1;
+    int powNum = 2;
+    int precision = TDDA_PREC_C128;
+    int verbose = 0;
+    AlphaParams ap{};
+    // host bookkeeping
+    long long nbox = 0;
+    std::vector<int32_t> geometry;
+    std::vector<long long> cell_of;       // dipole -> cell
+    std::vector<int> geometryPara;        // dipole -> parameter
+    std::vector<int> p2g_off, p2g_idx;    // parameter -> dipoles (CSR)
+    int NFpara = 0;
+    std::vector<double> parameters;
+    double E_int = 0.0;                   // objective state of the last calculateObjective
+    bool per_dipole = false;              // densities set per dipole (tdda_set_densities)
+    std::vector<double> rho_dipole;       // per-dipole densities when per_dipole
+    // device
+    cudaStream_t stream = nullptr;
+    ConvOperator<double2> op;
+    ConvOperator<float2> op32;
+    Krylov<double2> kv;
+    Krylov<float2> kv32;
+    int kv_nrhs = 0, kv32_nrhs = 0;
+    long long *d_cell = nullptr;
+    unsigned char *d_mask = nullptr;
+    double *d_rho = nullptr;        // density per cell
+    double2 *al = nullptr, *diel = nullptr;
+    float2 *al32 = nullptr;
+    double2 *Einc = nullptr;        // incident field [3][nbox]
+    double2 *P = nullptr;           // polarisation [3][nbox]
+    double2 *Eres = nullptr;        // EResult [3][nbox]
+    double2 *ext = nullptr;         // dipole-order staging, 3N (grows for batches)
+    long long ext_cap = 0;
+    double2 *bufB = nullptr, *bufX = nullptr;  // batch staging [nrhs][3][nbox]
+    int buf_nrhs = 0;
+    // mixed precision workspace
+    double2 *Rm = nullptr;
+    float2 *R32 = nullptr, *D32 = nullptr;
+    int mixed_nrhs = 0;
+    SolverState *st_res = nullptr, *st_res_host = nullptr;
+    double *d_part = nullptr, *h_part = nullptr;
+    // stats
+    double lattice_ms = 0, fft_ms = 0;
+    long long device_bytes = 0;
+
+    ~tdda_model() {
+        op.release();
+        op32.release();
+        kv.release();
+        kv32.release();
+        void *bufs[] = {d_cell, d_mask, d_rho, al, diel, al32, Einc, P, Eres, ext, bufB, bufX, Rm, R32, D32, st_res, d_part};
+        for (void *b : bufs) cudaFree(b);
+        cudaFreeHost(st_res_host);
+        cudaFreeHost(h_part);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+#define TRY(x)                                \
+    do {                                      \
+        tdda_status _s = (x);                 \
+        if (_s != TDDA_OK) return _s;         \
+    } while (0)
+
+static tdda_status bad(const std::string &msg) {
+    set_error(msg);
+    return TDDA_ERR_BAD_ARG;
+}
+
+static tdda_status ensure_ext(tdda_model *m, long long n) {
+    if (m->ext_cap >= n) return TDDA_OK;
+    cudaFree(m->ext);
+    m->ext = nullptr;
+    TDDA_CUDA_TRY(cudaMalloc(&m->ext, sizeof(double2) * n));
+    m->ext_cap = n;
+    return TDDA_OK;
+}
+
+static tdda_status ensure_batch(tdda_model *m, int nrhs) {
+    if (m->buf_nrhs >= nrhs) return TDDA_OK;
+    cudaFree(m->bufB);
+    cudaFree(m->bufX);
+    m->bufB = m->bufX = nullptr;
+    size_t bytes = sizeof(double2) * 3 * (size_t)m->nbox * nrhs;
+    TDDA_CUDA_TRY(cudaMalloc(&m->bufB, bytes));
+    TDDA_CUDA_TRY(cudaMalloc(&m->bufX, bytes));
+    if (m->N < m->nbox) {
+        TDDA_CUDA_TRY(cudaMemset(m->bufB, 0, bytes));
+        TDDA_CUDA_TRY(cudaMemset(m->bufX, 0, bytes));
+    }
+    m->buf_nrhs = nrhs;
+    return TDDA_OK;
+}
+
+static tdda_status ensure_op_cap(tdda_model *m, int nrhs) {
+    if (m->op.nrhs_cap >= nrhs) return TDDA_OK;
+    // grow the spectral intermediate and the reduction scratch
+    cudaFree(m->op.T);
+    m->op.T = nullptr;
+    TDDA_CUDA_TRY(cudaMalloc(&m->op.T, sizeof(double2) * (size_t)nrhs * 3 * m->op.g.tcomp));
+    cudaFree(m->op.partials);
+    cudaFree(m->op.counters);
+    m->op.partials = nullptr;
+    m->op.counters = nullptr;
+    TDDA_CUDA_TRY(cudaMalloc(&m->op.partials, sizeof(double2) * (size_t)m->op.partial_cap * nrhs));
+    TDDA_CUDA_TRY(cudaMalloc(&m->op.counters, sizeof(unsigned) * nrhs));
+    TDDA_CUDA_TRY(cudaMemset(m->op.counters, 0, sizeof(unsigned) * nrhs));
+    m->op.nrhs_cap = nrhs;
+    return TDDA_OK;
+}
+
+static tdda_status ensure_krylov(tdda_model *m, int nrhs) {
+    if (m->kv_nrhs < nrhs) {
+        m->kv.release();
+        TRY(m->kv.init(3 * m->nbox, nrhs));
+        if (m->N < m->nbox) {
+            size_t bytes = sizeof(double2) * 3 * (size_t)m->nbox * nrhs;
+            double2 *b[6] = {m->kv.r, m->kv.r0, m->kv.p, m->kv.t, m->kv.Ap, m->kv.At};
+            for (auto p : b) TDDA_CUDA_TRY(cudaMemset(p, 0, bytes));
+        }
+        m->kv_nrhs = nrhs;
+    }
+    return ensure_op_cap(m, nrhs);
+}
+
+static tdda_status ensure_mixed(tdda_model *m, int nrhs) {
+    if (m->kv32_nrhs < nrhs) {
+        m->kv32.release();
+        TRY(m->kv32.init(3 * m->nbox, nrhs));
+        if (m->N < m->nbox) {
+            size_t bytes = sizeof(float2) * 3 * (size_t)m->nbox * nrhs;
+            float2 *b[6] = {m->kv32.r, m->kv32.r0, m->kv32.p, m->kv32.t, m->kv32.Ap, m->kv32.At};
+            for (auto p : b) TDDA_CUDA_TRY(cudaMemset(p, 0, bytes));
+        }
+        m->kv32_nrhs = nrhs;
+    }
+    if (m->op32.nrhs_cap < nrhs) {
+        cudaFree(m->op32.T);
+        m->op32.T = nullptr;
+        TDDA_CUDA_TRY(cudaMalloc(&m->op32.T, sizeof(float2) * (size_t)nrhs * 3 * m->op32.g.tcomp));
+        cudaFree(m->op32.partials);
+        cudaFree(m->op32.counters);
+        TDDA_CUDA_TRY(cudaMalloc(&m->op32.partials, sizeof(double2) * (size_t)m->op32.partial_cap * nrhs));
+        TDDA_CUDA_TRY(cudaMalloc(&m->op32.counters, sizeof(unsigned) * nrhs));
+        TDDA_CUDA_TRY(cudaMemset(m->op32.counters, 0, sizeof(unsigned) * nrhs));
+        m->op32.nrhs_cap = nrhs;
+    }
+    if (m->mixed_nrhs < nrhs) {
+        cudaFree(m->Rm); cudaFree(m->R32); cudaFree(m->D32); cudaFree(m->st_res); cudaFreeHost(m->st_res_host);
+        m->Rm = nullptr; m->R32 = m->D32 = nullptr; m->st_res = nullptr; m->st_res_host = nullptr;
+        size_t n = 3 * (size_t)m->nbox * nrhs;
+        TDDA_CUDA_TRY(cudaMalloc(&m->Rm, sizeof(double2) * n));
+        TDDA_CUDA_TRY(cudaMalloc(&m->R32, sizeof(float2) * n));
+        TDDA_CUDA_TRY(cudaMalloc(&m->D32, sizeof(float2) * n));
+        TDDA_CUDA_TRY(cudaMemset(m->Rm, 0, sizeof(double2) * n));
+        TDDA_CUDA_TRY(cudaMemset(m->R32, 0, sizeof(float2) * n));
+        TDDA_CUDA_TRY(cudaMemset(m->D32, 0, sizeof(float2) * n));
+        TDDA_CUDA_TRY(cudaMalloc(&m->st_res, sizeof(SolverState) * nrhs));
+        TDDA_CUDA_TRY(cudaMallocHost(&m->st_res_host, sizeof(SolverState) * nrhs));
+        m->mixed_nrhs = nrhs;
+    }
+    return TDDA_OK;
+}
+
+static tdda_status update_alpha(tdda_model *m) {
+    // rho per cell from the parameters (src/DDAModel.cpp:762-770)
+    std::vector<double> rho(m->nbox, 0.0);
+    for (int i = 0; i < m->N; ++i)
+        rho[m->cell_of[i]] = m->per_dipole ? m->rho_dipole[i] : m->parameters[m->geometryPara[i]];
+    for (int i = 0; i < m->N; ++i) {
+        double v = rho[m->cell_of[i]];
+        if (!(v >= 0.0 && v <= 1.0)) return bad("design density outside [0, 1]");
+    }
+    TDDA_CUDA_TRY(cudaMemcpyAsync(m->d_rho, rho.data(), sizeof(double) * m->nbox, cudaMemcpyHostToDevice, m->stream));
+    count_launches(1);
+    k_alpha<<<grid_for(m->nbox), 256, 0, m->stream>>>(m->nbox, m->d_rho, m->d_mask, m->ap, m->al, m->al32, m->diel);
+    TDDA_CUDA_TRY(cudaGetLastError());
+    TDDA_CUDA_TRY(cudaStreamSynchronize(m->stream));
+    return TDDA_OK;
+}
+
+static tdda_status solve_c128(tdda_model *m, const double2 *B, double2 *X, int nrhs, bool x0_zero,
+                              int max_iter, double tol, tdda_solve_info *info) {
+    TRY(ensure_krylov(m, nrhs));
+    return bicgstab_device<double2>(m->op, m->kv, m->al, B, X, nrhs, x0_zero, max_iter, tol, m->stream, info,
+                                    nullptr);
+}
+
+// Mixed precision: complex64 BiCGSTAB on the normalised residual, complex128
+// residual and accumulation (iterative refinement) until ||B - A X||/||B|| <= tol.
+static tdda_status solve_mixed(tdda_model *m, const double2 *B, double2 *X, int nrhs, bool x0_zero,
+                               int max_iter, double tol, tdda_solve_info *info) {
+    TRY(ensure_mixed(m, nrhs));
+    const long long n = 3 * m->nbox;
+    if (x0_zero) TDDA_CUDA_TRY(cudaMemsetAsync(X, 0, sizeof(double2) * n * nrhs, m->stream));
+    std::vector<int> done(nrhs, 0), refine(nrhs, 0), inner(nrhs, 0);
+    std::vector<double> err(nrhs, 0.0);
+    std::vector<int> status(nrhs, TDDA_SOLVE_RUNNING);
+    const int max_refine = 12;
+    for (int outer = 0; outer <= max_refine; ++outer) {
+        TRY(residual_c128(m->op, m->al, B, X, m->Rm, m->st_res, nrhs, m->stream));
+        TDDA_CUDA_TRY(cudaMemcpyAsync(m->st_res_host, m->st_res, sizeof(SolverState) * nrhs, cudaMemcpyDeviceToHost, m->stream));
+        TDDA_CUDA_TRY(cudaStreamSynchronize(m->stream));
+        bool all = true;
+        for (int k = 0; k < nrhs; ++k) {
+            if (done[k]) continue;
+            const SolverState &S = m->st_res_host[k];
+            err[k] = S.err;
+            if (S.enorm == 0.0) {
+                TDDA_CUDA_TRY(cudaMemsetAsync(X + (size_t)k * n, 0, sizeof(double2) * n, m->stream));
+                done[k] = 1; status[k] = TDDA_SOLVE_ZERO_RHS; err[k] = 0.0;
+            } else if (S.err <= tol) {
+                done[k] = 1; status[k] = TDDA_SOLVE_CONVERGED;
+            } else if (!std::isfinite(S.err)) {
+                done[k] = 1; status[k] = TDDA_SOLVE_NONFINITE;
+            } else if (outer == max_refine || inner[k] >= max_iter) {
+                done[k] = 1; status[k] = TDDA_SOLVE_MAXITER;
+            }
+            all &= (done[k] != 0);
+        }
+        if (all) break;
+        // one batched complex64 solve over every unfinished right-hand side,
+        // each normalised by its own residual norm (finished ones get a zero RHS)
+        std::vector<double> h(3 * (size_t)nrhs, 0.0);
+        int budget = 1;
+        for (int k = 0; k < nrhs; ++k) {
+            if (done[k]) continue;
+            const SolverState &S = m->st_res_host[k];
+            const double rn = S.err * S.enorm;
+            h[k] = 1.0 / rn;                                   // scale into the inner RHS
+            h[nrhs + k] = rn;                                  // scale of the correction
+            h[2 * nrhs + k] = std::max(0.5 * tol / S.err, 2e-6);  // inner tolerance
+            budget = std::max(budget, max_iter - inner[k]);
+        }
+        TDDA_CUDA_TRY(cudaMemcpyAsync(m->d_part, h.data(), sizeof(double) * 3 * nrhs, cudaMemcpyHostToDevice, m->stream));
+        count_launches(1);
+        k_to32_batch<<<grid_for(n * nrhs), 256, 0, m->stream>>>(n, nrhs, m->Rm, m->d_part, m->R32);
+        std::vector<tdda_solve_info> ii(nrhs);
+        TRY(bicgstab_device<float2>(m->op32, m->kv32, m->al32, m->R32, m->D32, nrhs, true, budget,
+                                    h[2 * nrhs], m->stream, ii.data(), h.data() + 2 * nrhs));
+        count_launches(1);
+        k_axpy32_batch<<<grid_for(n * nrhs), 256, 0, m->stream>>>(n, nrhs, m->d_part + nrhs, m->D32, X);
+        TDDA_CUDA_TRY(cudaGetLastError());
+        for (int k = 0; k < nrhs; ++k) {
+            if (done[k]) continue;
+            inner[k] += ii[k].iterations;
+            refine[k] += 1;
+        }
+    }
+    if (info)
+        for (int k = 0; k < nrhs; ++k) {
+            info[k].iterations = inner[k];
+            info[k].error = err[k];
+            info[k].status = status[k];
+            info[k].refinements = refine[k];
+            info[k].inner_iterations = inner[k];
+            info[k].true_error = err[k];
+        }
+    return TDDA_OK;
+}
+
+static tdda_status solve_internal(tdda_model *m, const double2 *B, double2 *X, int nrhs, bool x0_zero,
+                                  int max_iter, double tol, tdda_solve_info *info) {
+    if (max_iter < 0) return bad("max_iter must be >= 0");
+    if (!(tol >= 0.0)) return bad("tolerance must be >= 0");
+    if (m->precision == TDDA_PREC_MIXED) return solve_mixed(m, B, X, nrhs, x0_zero, max_iter, tol, info);
+    return solve_c128(m, B, X, nrhs, x0_zero, max_iter, tol, info);
+}
+
+// ----------------------------------------------------------------------------
+// C ABI
+// ----------------------------------------------------------------------------
+extern "C" {
+
+const char *tdda_status_string(tdda_status s) {
+    switch (s) {
+        case TDDA_OK: return "ok";
+        case TDDA_ERR_BAD_ARG: return "bad argument";
+        case TDDA_ERR_OOM: return "out of device memory";
+        case TDDA_ERR_NOT_CONVERGED: return "not converged";
+        case TDDA_ERR_BREAKDOWN: return "breakdown";
+        case TDDA_ERR_CUDA: return "CUDA error";
+        case TDDA_ERR_TIMEOUT: return "timeout";
+        case TDDA_ERR_UNSUPPORTED: return "unsupported";
+        case TDDA_ERR_STATE: return "invalid state";
+    }
+    return "unknown";
+}
+
+const char *tdda_last_error(void) { return get_error(); }
+int tdda_abi_version(void) { return 1; }
+
+tdda_status tdda_model_create(const tdda_params *p, const int32_t *geometry, const double *input_dielectrics,
+                              const double *si, const double *ci, int64_t ntab, tdda_model **out) {
+    if (out == nullptr || p == nullptr || geometry == nullptr || input_dielectrics == nullptr)
+        return bad("null argument");
+    *out = nullptr;
+    std::unique_ptr<tdda_model> m(new tdda_model());
+    m->Nx = p->num_x; m->Ny = p->num_y; m->Nz = p->num_z; m->N = p->num_total;
+    if (m->Nx < 1 || m->Ny < 1 || m->Nz < 1 || m->N < 1) return bad("grid sizes must be positive");
+    m->nbox = (long long)m->Nx * m->Ny * m->Nz;
+    if (m->N > m->nbox) return bad("num_total exceeds num_x*num_y*num_z");
+    if (p->d <= 0 || p->lam <= 0 || p->nback <= 0) return bad("d, lam and nback must be positive");
+    if (p->use_filter) return bad("useFilter=true: the legacy density filter is not part of this path");
+    std::string sym = p->symmetry_type ? p->symmetry_type : "";
+    int dividesym;
+    if (sym == "None") dividesym = 1;
+    else if (sym == "4fold") dividesym = 4;
+    else return bad("symmetryType must be \"None\" or \"4fold\" (src/DDAModel.cpp:163-173)");
+    std::string meth = p->matrix_method ? p->matrix_method : "";
+    if (meth == "FCD") m->method = 0;
+    else if (meth == "LDR") m->method = 1;
+    else return bad("\"" + meth + "\" is not a valid polarizabiliy calculation method.");
+    if (m->method == 0 && (si == nullptr || ci == nullptr || ntab < 2)) return bad("FCD needs SiCi tables");
+    if (p->n_obj_para < 1 || p->obj_para == nullptr) return bad("objPara needs at least the power");
+    if (p->MAXm < 0 || p->MAXn < 0) return bad("MAXm, MAXn must be >= 0");
+    m->powNum = (int)std::lround(p->obj_para[0]);
+    m->d = p->d; m->lam = p->lam; m->nback = p->nback; m->E0 = p->E0;
+    for (int c = 0; c < 3; ++c) { m->nK[c] = p->n_K[c]; m->nE0[c] = p->n_E0[c]; }
+    m->MAXm = p->MAXm; m->MAXn = p->MAXn;
+    m->Lm = p->Lm * p->d; m->Ln = p->Ln * p->d;
+    m->delta = p->integral_delta;
+    m->precision = p->precision;
+    m->verbose = p->verbose;
+    // src/AProductCore.cpp:25-33: K, rescale materials
+    m->K = 2.0 * M_PI / (m->lam / m->nback);
+    for (int i = 0; i < 2; ++i) {
+        std::complex<double> v(p->material[2 * i], p->material[2 * i + 1]);
+        v = v / (m->nback * m->nback);
+        if (std::sqrt(std::norm(v)) < 1.01) v = v + 0.01;
+        m->mat[i] = make_double2(v.real(), v.imag());
+    }
+    m->ap.lam = m->lam; m->ap.K = m->K; m->ap.d = m->d; m->ap.m0 = m->mat[0]; m->ap.m1 = m->mat[1];
+    m->ap.S = std::pow(m->nE0[0] * m->nK[0], 2) + std::pow(m->nE0[1] * m->nK[1], 2) + std::pow(m->nE0[2] * m->nK[2], 2);
+    // geometry -> cells
+    m->geometry.assign(geometry, geometry + 3 * (size_t)m->N);
+    m->cell_of.resize(m->N);
+    std::vector<unsigned char> mask(m->nbox, 0);
+    for (int i = 0; i < m->N; ++i) {
+        int x = geometry[3 * i], y = geometry[3 * i + 1], z = geometry[3 * i + 2];
+        if (x < 0 || x >= m->Nx || y < 0 || y >= m->Ny || z < 0 || z >= m->Nz)
+            return bad("geometry coordinate outside the num_x*num_y*num_z box");
+        long long cell = ((long long)x * m->Ny + y) * m->Nz + z;
+        if (mask[cell]) return bad("duplicate geometry coordinate");
+        mask[cell] = 1;
+        m->cell_of[i] = cell;
+    }
+    // parameter map (src/DDAModel.cpp:181-247, FCurrentinsert :37-64)
+    m->NFpara = (int)std::lround((double)(3 * m->N / 3 / m->Nz / dividesym));
+    std::map<std::pair<int, int>, int> cur;
+    int pos = 0;
+    m->geometryPara.resize(m->N);
+    for (int i = 0; i < m->N; ++i) {
+        std::pair<int, int> xy(geometry[3 * i], geometry[3 * i + 1]);
+        auto it = cur.find(xy);
+        if (it == cur.end()) {
+            if (dividesym == 1) {
+                cur[xy] = pos++;
+            } else {
+                auto mir = [](double ax, int v) { return (int)std::lround(2 * ax - v); };
+                std::pair<int, int> s1(mir(p->symmetry_axis[0], xy.first), xy.second);
+                std::pair<int, int> s2(mir(p->symmetry_axis[0], xy.first), mir(p->symmetry_axis[1], xy.second));
+                std::pair<int, int> s3(xy.first, mir(p->symmetry_axis[1], xy.second));
+                if (cur.count(s1)) cur[xy] = cur[s1];
+                else if (cur.count(s2)) cur[xy] = cur[s2];
+                else if (cur.count(s3)) cur[xy] = cur[s3];
+                else cur[xy] = pos++;
+            }
+        }
+        m->geometryPara[i] = cur[xy];
+    }
+    if (pos != m->NFpara)
+        return bad("symmetry map yields " + std::to_string(pos) + " free parameters, expected NFpara=" +
+                   std::to_string(m->NFpara));
+    m->p2g_off.assign(m->NFpara + 1, 0);
+    for (int i = 0; i < m->N; ++i) m->p2g_off[m->geometryPara[i] + 1]++;
+    for (int k = 0; k < m->NFpara; ++k) m->p2g_off[k + 1] += m->p2g_off[k];
+    m->p2g_idx.resize(m->N);
+    {
+        std::vector<int> fill(m->p2g_off.begin(), m->p2g_off.end() - 1);
+        for (int i = 0; i < m->N; ++i) m->p2g_idx[fill[m->geometryPara[i]]++] = i;
+    }
+    // initial parameters: value of the first dipole of each parameter (src/DDAModel.cpp:227-247)
+    m->parameters.resize(m->NFpara);
+    for (int k = 0; k < m->NFpara; ++k) m->parameters[k] = input_dielectrics[3 * (size_t)m->p2g_idx[m->p2g_off[k]]];
+
+    // device state
+    TDDA_CUDA_TRY(cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking));
+    TRY(m->op.init(m->Nx, m->Ny, m->Nz, 1));
+    const ConvGeom &g = m->op.g;
+    const size_t nfold = (size_t)g.hx * g.hy * g.hz * 6;
+    TDDA_CUDA_TRY(cudaMalloc(&m->op.ahat, sizeof(double2) * nfold));
+    float2 *ahat32 = nullptr;
+    if (m->precision == TDDA_PREC_MIXED) {
+        TRY(m->op32.init(m->Nx, m->Ny, m->Nz, 1));
+        TDDA_CUDA_TRY(cudaMalloc(&m->op32.ahat, sizeof(float2) * nfold));
+        ahat32 = m->op32.ahat;
+    } else if (m->precision != TDDA_PREC_C128) {
+        return bad("precision must be 0 (complex128) or 1 (mixed)");
+    }
+    const bool full = (m->N == m->nbox);
+    if (!full) {
+        TDDA_CUDA_TRY(cudaMalloc(&m->d_mask, m->nbox));
+        TDDA_CUDA_TRY(cudaMemcpy(m->d_mask, mask.data(), m->nbox, cudaMemcpyHostToDevice));
+        m->op.mask = m->d_mask;
+        m->op32.mask = m->d_mask;
+    }
+    TDDA_CUDA_TRY(cudaMalloc(&m->d_cell, sizeof(long long) * m->N));
+    TDDA_CUDA_TRY(cudaMemcpy(m->d_cell, m->cell_of.data(), sizeof(long long) * m->N, cudaMemcpyHostToDevice));
+    TDDA_CUDA_TRY(cudaMalloc(&m->d_rho, sizeof(double) * m->nbox));
+    TDDA_CUDA_TRY(cudaMemset(m->d_rho, 0, sizeof(double) * m->nbox));
+    TDDA_CUDA_TRY(cudaMalloc(&m->al, sizeof(double2) * m->nbox));
+    TDDA_CUDA_TRY(cudaMalloc(&m->diel, sizeof(double2) * m->nbox));
+    if (m->precision == TDDA_PREC_MIXED) TDDA_CUDA_TRY(cudaMalloc(&m->al32, sizeof(float2) * m->nbox));
+    const size_t nvec = 3 * (size_t)m->nbox;
+    TDDA_CUDA_TRY(cudaMalloc(&m->Einc, sizeof(double2) * nvec));
+    TDDA_CUDA_TRY(cudaMalloc(&m->P, sizeof(double2) * nvec));
+    TDDA_CUDA_TRY(cudaMalloc(&m->Eres, sizeof(double2) * nvec));
+    TDDA_CUDA_TRY(cudaMemset(m->Einc, 0, sizeof(double2) * nvec));
+    TDDA_CUDA_TRY(cudaMemset(m->P, 0, sizeof(double2) * nvec));
+    TDDA_CUDA_TRY(cudaMemset(m->Eres, 0, sizeof(double2) * nvec));
+    TDDA_CUDA_TRY(cudaMalloc(&m->d_part, sizeof(double) * 1024));
+    TDDA_CUDA_TRY(cudaMallocHost(&m->h_part, sizeof(double) * 1024));
+    TRY(ensure_ext(m.get(), 3 * (long long)m->N));
+
+    // interaction tensor
+    LatticeParams L{};
+    L.nx = m->Nx; L.ny = m->Ny; L.nz = m->Nz;
+    L.Lx = g.Lx; L.Ly = g.Ly; L.Lz = g.Lz;
+    L.d = m->d; L.K = m->K; L.Kf = M_PI / m->d; L.Lm = m->Lm; L.Ln = m->Ln;
+    L.MAXm = m->MAXm; L.MAXn = m->MAXn; L.method = m->method; L.gamma = 0.01; L.delta = m->delta;
+    std::vector<double> dummy(2, 0.0);
+    const double *tsi = si ? si : dummy.data(), *tci = ci ? ci : dummy.data();
+    long nt = (si && ci) ? (long)ntab : 2;
+    TRY(build_tensor(L, tsi, tci, nt, m->op.ahat, ahat32, m->stream, &m->lattice_ms, &m->fft_ms));
+
+    // incident field (src/DDAModel.cpp:312-316), internal layout
+    {
+        std::vector<double2> e(nvec, make_double2(0.0, 0.0));
+        for (int i = 0; i < m->N; ++i) {
+            const int32_t *gi = &geometry[3 * i];
+            double ph = m->K * m->d * (m->nK[0] * gi[0] + m->nK[1] * gi[1] + m->nK[2] * gi[2]);
+            double cr = std::cos(ph), sn = std::sin(ph);
+            for (int c = 0; c < 3; ++c)
+                e[(size_t)c * m->nbox + m->cell_of[i]] = make_double2(m->E0 * m->nE0[c] * cr, m->E0 * m->nE0[c] * sn);
+        }
+        TDDA_CUDA_TRY(cudaMemcpy(m->Einc, e.data(), sizeof(double2) * nvec, cudaMemcpyHostToDevice));
+    }
+    TRY(update_alpha(m.get()));
+    size_t fr = 0, tot = 0;
+    cudaMemGetInfo(&fr, &tot);
+    m->device_bytes = (long long)(sizeof(double2) * nfold + sizeof(double2) * nvec * 3 +
+                                  sizeof(double2) * 3 * g.tcomp);
+    *out = m.release();
+    return TDDA_OK;
+}
+
+void tdda_model_destroy(tdda_model *m) { delete m; }
+
+tdda_status tdda_model_get_info(const tdda_model *m, tdda_model_info *info) {
+    if (!m || !info) return bad("null argument");
+    info->N = m->N; info->NFpara = m->NFpara;
+    info->nx = m->Nx; info->ny = m->Ny; info->nz = m->Nz;
+    info->Lx = m->op.g.Lx; info->Ly = m->op.g.Ly; info->Lz = m->op.g.Lz;
+    info->K = m->K;
+    for (int i = 0; i < 2; ++i) { info->material[2 * i] = m->mat[i].x; info->material[2 * i + 1] = m->mat[i].y; }
+    info->device_bytes = m->device_bytes;
+    info->lattice_ms = m->lattice_ms;
+    info->tensor_fft_ms = m->fft_ms;
+    return TDDA_OK;
+}
+
+static tdda_status to_internal(tdda_model *m, const double *host, double2 *dst, int nrhs) {
+    const long long n = 3 * (long long)m->N * nrhs;
+    TRY(ensure_ext(m, n));
+    TDDA_CUDA_TRY(cudaMemcpyAsync(m->ext, host, sizeof(double2) * n, cudaMemcpyHostToDevice, m->stream));
+    count_launches(1);
+    k_scatter<<<grid_for(n), 256, 0, m->stream>>>(nrhs, m->N, m->nbox, m->d_cell, m->ext, dst);
+    TDDA_CUDA_TRY(cudaGetLastError());
+    return TDDA_OK;
+}
+
+static tdda_status to_host(tdda_model *m, const double2 *src, double *host, int nrhs) {
+    const long long n = 3 * (long long)m->N * nrhs;
+    TRY(ensure_ext(m, n));
+    count_launches(1);
+    k_gather<<<grid_for(n), 256, 0, m->stream>>>(nrhs, m->N, m->nbox, m->d_cell, src, m->ext);
+    TDDA_CUDA_TRY(cudaGetLastError());
+    TDDA_CUDA_TRY(cudaMemcpyAsync(host, m->ext, sizeof(double2) * n, cudaMemcpyDeviceToHost, m->stream));
+    TDDA_CUDA_TRY(cudaStreamSynchronize(m->stream));
+    return TDDA_OK;
+}
+
+tdda_status tdda_solve_electric_field(tdda_model *m, const double *P0, int max_iter, double tol,
+                                      tdda_solve_info *info) {
+    if (!m) return bad("null model");
+    bool zero = (P0 == nullptr);
+    if (!zero) {
+        zero = true;
+        for (long long i = 0; i < 6LL * m->N && zero; ++i) zero = (P0[i] == 0.0);
+        if (!zero) TRY(to_internal(m, P0, m->P, 1));
+    }
+    tdda_solve_info inf{};
+    TRY(solve_internal(m, m->Einc, m->P, 1, zero, max_iter, tol, &inf));
+    count_launches(1);
+    k_eresult<<<grid_for(3 * m->nbox), 256, 0, m->stream>>>(m->nbox, m->P, m->al, m->diel, m->Eres);
+    TDDA_CUDA_TRY(cudaGetLastError());
+    TDDA_CUDA_TRY(cudaStreamSynchronize(m->stream));
+    if (m->verbose)
+        fprintf(stderr, "[tdda] solve: %d iterations, error %.3e, status %d\n", inf.iterations, inf.error, inf.status);
+    if (info) *info = inf;
+    return TDDA_OK;
+}
+
+static tdda_status objective_sum(tdda_model *m, const double2 *P, double *S) {
+    const int nb = 512;
+    count_launches(1);
+    k_objective<<<nb, 256, 0, m->stream>>>(m->nbox, P, m->al, m->d_mask, m->powNum, m->d_part);
+    TDDA_CUDA_TRY(cudaGetLastError());
+    TDDA_CUDA_TRY(cudaMemcpyAsync(m->h_part, m->d_part, sizeof(double) * nb, cudaMemcpyDeviceToHost, m->stream));
+    TDDA_CUDA_TRY(cudaStreamSynchronize(m->stream));
+    double s = 0.0;
+    for (int b = 0; b < nb; ++b) s += m->h_part[b];
+    *S = s;
+    return TDDA_OK;
+}
+
+tdda_status tdda_calculate_objective(tdda_model *m, double *out) {
+    if (!m || !out) return bad("null argument");
+    double S;
+    TRY(objective_sum(m, m->P, &S));
+    m->E_int = S;
+    *out = std::log(S);
+    return TDDA_OK;
+}
+
+tdda_status tdda_calculate_gradients(tdda_model *m, double eps, double J0, int max_iter, double tol, double *grad,
+                                     int64_t n) {
+    if (!m || !grad) return bad("null argument");
+    if (n != m->NFpara) return bad("gradient buffer must hold NFpara values");
+    if (!(eps != 0.0)) return bad("epsilon_partial must be non-zero");
+    if (m->per_dipole) {
+        set_error("densities were set per dipole: use tdda_gradient_densities");
+        return TDDA_ERR_STATE;
+    }
+    const long long nbox = m->nbox;
+    TRY(ensure_batch(m, 1));
+    double *dS = nullptr;
+    double2 *change = nullptr, *prod = nullptr;
+    TDDA_CUDA_TRY(cudaMalloc(&dS, sizeof(double) * nbox));
+    std::unique_ptr<void, void (*)(void *)> g1(dS, [](void *p) { cudaFree(p); });
+    TDDA_CUDA_TRY(cudaMalloc(&change, sizeof(double2) * nbox));
+    std::unique_ptr<void, void (*)(void *)> g2(change, [](void *p) { cudaFree(p); });
+    TDDA_CUDA_TRY(cudaMalloc(&prod, sizeof(double2) * nbox));
+    std::unique_ptr<void, void (*)(void *)> g3(prod, [](void *p) { cudaFree(p); });
+    GradFD G{m->ap, eps, J0, m->E_int, m->powNum};
+    double2 *devp = m->bufB;
+    count_launches(1);
+    k_grad_fd<<<grid_for(nbox), 256, 0, m->stream>>>(nbox, m->d_rho, m->d_mask, m->P, m->al, G, dS, change, devp);
+    TDDA_CUDA_TRY(cudaGetLastError());
+    std::vector<double> hdS(nbox);
+    TDDA_CUDA_TRY(cudaMemcpyAsync(hdS.data(), dS, sizeof(double) * nbox, cudaMemcpyDeviceToHost, m->stream));
+    // adjoint solve with the same complex-symmetric operator (src/DDAModel.cpp:429-435)
+    double2 *lam = m->bufX;
+    tdda_solve_info inf{};
+    TRY(solve_internal(m, devp, lam, 1, true, max_iter, tol, &inf));
+    count_launches(1);
+    k_grad_mult<<<grid_for(nbox), 256, 0, m->stream>>>(nbox, lam, m->P, change, prod);
+    TDDA_CUDA_TRY(cudaGetLastError());
+    std::vector<double2> hprod(nbox);
+    TDDA_CUDA_TRY(cudaMemcpyAsync(hprod.data(), prod, sizeof(double2) * nbox, cudaMemcpyDeviceToHost, m->stream));
+    TDDA_CUDA_TRY(cudaStreamSynchronize(m->stream));
+    for (int k = 0; k < m->NFpara; ++k) {
+        const double rho = m->parameters[k];
+        const double se = (rho >= eps ? -1.0 : 1.0) * eps;
+        double dsum = 0.0, mult = 0.0;
+        for (int q = m->p2g_off[k]; q < m->p2g_off[k + 1]; ++q) {
+            long long cell = m->cell_of[m->p2g_idx[q]];
+            dsum += hdS[cell];
+            mult += hprod[cell].x;
+        }
+        const double devx = (std::log(m->E_int + dsum) - J0) / se;
+        grad[k] = devx - mult;
+    }
+    // as in the reference, the model's polarisation now holds the adjoint solution
+    TDDA_CUDA_TRY(cudaMemcpyAsync(m->P, lam, sizeof(double2) * 3 * nbox, cudaMemcpyDeviceToDevice, m->stream));
+    TDDA_CUDA_TRY(cudaStreamSynchronize(m->stream));
+    if (m->verbose)
+        fprintf(stderr, "[tdda] adjoint: %d iterations, error %.3e\n", inf.iterations, inf.error);
+    return TDDA_OK;
+}
+
+tdda_status tdda_set_parameters(tdda_model *m, const double *values, int64_t n) {
+    if (!m || !values) return bad("null argument");
+    if (n != m->NFpara) return bad("ERROR: In CoreStructure::UpdateStr(VectorXd step), step.size!=FreePara.size");
+    std::vector<double> old = m->parameters;
+    const bool old_pd = m->per_dipole;
+    m->parameters.assign(values, values + n);
+    m->per_dipole = false;
+    tdda_status s = update_alpha(m);
+    if (s != TDDA_OK) {
+        m->parameters = old;
+        m->per_dipole = old_pd;
+    }
+    return s;
+}
+
+tdda_status tdda_get_parameters(const tdda_model *m, double *out, int64_t n) {
+    if (!m || !out) return bad("null argument");
+    if (n != m->NFpara) return bad("buffer must hold NFpara values");
+    std::copy(m->parameters.begin(), m->parameters.end(), out);
+    return TDDA_OK;
+}
+
+tdda_status tdda_get_dielectrics(const tdda_model *m, double *out, int64_t n) {
+    if (!m || !out) return bad("null argument");
+    if (n != 3LL * m->N) return bad("buffer must hold 3N values");
+    for (int i = 0; i < m->N; ++i) {
+        double v = m->per_dipole ? m->rho_dipole[i] : m->parameters[m->geometryPara[i]];
+        out[3 * i] = out[3 * i + 1] = out[3 * i + 2] = v;
+    }
+    return TDDA_OK;
+}
+
+tdda_status tdda_get_electric_field(const tdda_model *m, double *out, int64_t n) {
+    if (!m || !out) return bad("null argument");
+    if (n != 3LL * m->N) return bad("buffer must hold 3N complex values");
+    return to_host(const_cast<tdda_model *>(m), m->Eres, out, 1);
+}
+
+tdda_status tdda_get_polarization(const tdda_model *m, double *out, int64_t n) {
+    if (!m || !out) return bad("null argument");
+    if (n != 3LL * m->N) return bad("buffer must hold 3N complex values");
+    return to_host(const_cast<tdda_model *>(m), m->P, out, 1);
+}
+
+tdda_status tdda_matvec(tdda_model *m, const double *x, double *y, int with_al) {
+    if (!m || !x || !y) return bad("null argument");
+    TRY(ensure_batch(m, 1));
+    TRY(to_internal(m, x, m->bufB, 1));
+    TRY(m->op.apply(m->bufB, m->bufX, with_al ? m->al : nullptr, 1, m->stream));
+    return to_host(m, m->bufX, y, 1);
+}
+
+tdda_status tdda_solve_batch_device(tdda_model *m, const void *B_dev, void *X_dev, int nrhs, int x0_zero,
+                                    int max_iter, double tol, void *stream, tdda_solve_info *infos) {
+    if (!m || !X_dev || nrhs < 1) return bad("bad argument");
+    cudaStream_t user = (cudaStream_t)stream;
+    cudaEvent_t ev;
+    TDDA_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    std::unique_ptr<CUevent_st, void (*)(cudaEvent_t)> evg(ev, [](cudaEvent_t e) { cudaEventDestroy(e); });
+    // order the model stream after the caller's stream
+    TDDA_CUDA_TRY(cudaEventRecord(ev, user));
+    TDDA_CUDA_TRY(cudaStreamWaitEvent(m->stream, ev, 0));
+    TRY(ensure_batch(m, nrhs));
+    const long long n3 = 3 * (long long)m->N;
+    const size_t nvec = 3 * (size_t)m->nbox;
+    if (B_dev) {
+        count_launches(1);
+        k_scatter<<<grid_for(n3 * nrhs), 256, 0, m->stream>>>(nrhs, m->N, m->nbox, m->d_cell,
+                                                             (const double2 *)B_dev, m->bufB);
+    } else {
+        for (int k = 0; k < nrhs; ++k)
+            TDDA_CUDA_TRY(cudaMemcpyAsync(m->bufB + k * nvec, m->Einc, sizeof(double2) * nvec,
+                                          cudaMemcpyDeviceToDevice, m->stream));
+    }
+    if (!x0_zero) {
+        count_launches(1);
+        k_scatter<<<grid_for(n3 * nrhs), 256, 0, m->stream>>>(nrhs, m->N, m->nbox, m->d_cell,
+                                                             (const double2 *)X_dev, m->bufX);
+    }
+    TDDA_CUDA_TRY(cudaGetLastError());
+    TRY(solve_internal(m, m->bufB, m->bufX, nrhs, x0_zero != 0, max_iter, tol, infos));
+    count_launches(1);
+    k_gather<<<grid_for(n3 * nrhs), 256, 0, m->stream>>>(nrhs, m->N, m->nbox, m->d_cell, m->bufX, (double2 *)X_dev);
+    TDDA_CUDA_TRY(cudaGetLastError());
+    TDDA_CUDA_TRY(cudaEventRecord(ev, m->stream));
+    TDDA_CUDA_TRY(cudaStreamWaitEvent(user, ev, 0));
+    return TDDA_OK;
+}
+
+tdda_status tdda_matvec_device(tdda_model *m, const void *x_dev, void *y_dev, int nrhs, int with_al, void *stream) {
+    if (!m || !x_dev || !y_dev || nrhs < 1) return bad("bad argument");
+    cudaStream_t user = (cudaStream_t)stream;
+    cudaEvent_t ev;
+    TDDA_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    std::unique_ptr<CUevent_st, void (*)(cudaEvent_t)> evg(ev, [](cudaEvent_t e) { cudaEventDestroy(e); });
+    TDDA_CUDA_TRY(cudaEventRecord(ev, user));
+    TDDA_CUDA_TRY(cudaStreamWaitEvent(m->stream, ev, 0));
+    TRY(ensure_batch(m, nrhs));
+    TRY(ensure_op_cap(m, nrhs));
+    const long long n3 = 3 * (long long)m->N;
+    count_launches(1);
+    k_scatter<<<grid_for(n3 * nrhs), 256, 0, m->stream>>>(nrhs, m->N, m->nbox, m->d_cell, (const double2 *)x_dev, m->bufB);
+    TRY(m->op.apply(m->bufB, m->bufX, with_al ? m->al : nullptr, nrhs, m->stream));
+    count_launches(1);
+    k_gather<<<grid_for(n3 * nrhs), 256, 0, m->stream>>>(nrhs, m->N, m->nbox, m->d_cell, m->bufX, (double2 *)y_dev);
+    TDDA_CUDA_TRY(cudaGetLastError());
+    TDDA_CUDA_TRY(cudaEventRecord(ev, m->stream));
+    TDDA_CUDA_TRY(cudaStreamWaitEvent(user, ev, 0));
+    return TDDA_OK;
+}
+
+tdda_status tdda_set_densities(tdda_model *m, const double *rho, int64_t n) {
+    if (!m || !rho) return bad("null argument");
+    if (n != m->N) return bad("densities must hold N values");
+    std::vector<double> old = m->rho_dipole;
+    const bool old_pd = m->per_dipole;
+    m->rho_dipole.assign(rho, rho + n);
+    m->per_dipole = true;
+    tdda_status s = update_alpha(m);
+    if (s != TDDA_OK) {
+        m->rho_dipole = old;
+        m->per_dipole = old_pd;
+    }
+    return s;
+}
+
+tdda_status tdda_gradient_densities(tdda_model *m, int max_iter, double tol, double *grad, int64_t n,
+                                    tdda_solve_info *info) {
+    if (!m || !grad) return bad("null argument");
+    if (n != m->N) return bad("gradient buffer must hold N values");
+    double S;
+    TRY(objective_sum(m, m->P, &S));
+    if (!(S > 0.0)) return bad("objective sum is zero: solve first");
+    TRY(ensure_batch(m, 1));
+    const long long nbox = m->nbox;
+    k_adjoint_rhs<<<grid_for(nbox), 256, 0, m->stream>>>(nbox, m->P, m->al, m->d_mask, m->powNum, S, m->bufB);
+    count_launches(1);
+    TDDA_CUDA_TRY(cudaGetLastError());
+    tdda_solve_info inf{};
+    TRY(solve_internal(m, m->bufB, m->bufX, 1, true, max_iter, tol, &inf));
+    double *g = nullptr;
+    TDDA_CUDA_TRY(cudaMalloc(&g, sizeof(double) * nbox));
+    std::unique_ptr<void, void (*)(void *)> gg(g, [](void *p) { cudaFree(p); });
+    k_grad_analytic<<<grid_for(nbox), 256, 0, m->stream>>>(nbox, m->d_rho, m->d_mask, m->P, m->al, m->diel, m->bufX,
+                                                           m->ap, m->powNum, S, g);
+    count_launches(1);
+    TDDA_CUDA_TRY(cudaGetLastError());
+    std::vector<double> h(nbox);
+    TDDA_CUDA_TRY(cudaMemcpyAsync(h.data(), g, sizeof(double) * nbox, cudaMemcpyDeviceToHost, m->stream));
+    TDDA_CUDA_TRY(cudaStreamSynchronize(m->stream));
+    for (int i = 0; i < m->N; ++i) grad[i] = h[m->cell_of[i]];
+    if (info) *info = inf;
+    return TDDA_OK;
+}
+
+tdda_status tdda_profile_matvec(tdda_model *m, int precision, int nrhs, int iters, double *ms_matvec,
+                                double *ms_pass) {
+    if (!m || !ms_matvec || !ms_pass || nrhs < 1) return bad("bad argument");
+    if (precision == 0) {
+        TRY(ensure_batch(m, nrhs));
+        TRY(ensure_op_cap(m, nrhs));
+        return profile_apply<double2>(m->op, m->bufB, m->bufX, m->al, nrhs, iters, m->stream, ms_matvec, ms_pass);
+    }
+    if (m->precision != TDDA_PREC_MIXED) {
+        set_error("complex64 operator exists only in mixed-precision models");
+        return TDDA_ERR_UNSUPPORTED;
+    }
+    TRY(ensure_mixed(m, nrhs));
+    return profile_apply<float2>(m->op32, m->kv32.r, m->kv32.p, m->al32, nrhs, iters, m->stream, ms_matvec, ms_pass);
+}
+
+long long tdda_kernel_launches(void) { return launches_total(); }
+
+tdda_status tdda_set_precision(tdda_model *m, int precision) {
+    if (!m) return bad("null model");
+    if (precision == TDDA_PREC_C128) { m->precision = TDDA_PREC_C128; return TDDA_OK; }
+    if (precision == TDDA_PREC_MIXED) {
+        if (m->op32.ahat == nullptr) {
+            set_error("model was created in complex128: no complex64 operator");
+            return TDDA_ERR_STATE;
+        }
+        m->precision = TDDA_PREC_MIXED;
+        return TDDA_OK;
+    }
+    return bad("precision must be 0 or 1");
+}
+
+}  // extern "C"

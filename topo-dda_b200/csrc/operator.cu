@@ -1,0 +1,811 @@
+// Fused zero-padded FFT convolution A.x and the BiCGSTAB built on it.
+//
+// One application of the interaction operator runs as three kernels:
+//   pass 1  k_fwd_zy : per (x-slab, component): load the ny*nz slab (with a
+//            fused prologue that can form the slab from several solver
+//            vectors), z-FFT (zero padded), y-FFT (zero padded), store the
+//            populated x-half of the spectrum to T.
+//   pass 2  k_xconv  : per (ky, kz-chunk): x-FFT of all three components of
+//            every right-hand side, symmetric 3x3 multiply by the cached
+//            folded Green-tensor spectrum, inverse x-FFT, store back to T
+//            (only x < nx is kept).
+//   pass 3  k_inv_yz : per (x-slab, component): inverse y-FFT, crop y < ny,
+//            inverse z-FFT, crop z < nz, fused epilogue (polarisability
+//            diagonal, residual / vector updates, dot products with a
+//            deterministic last-block reduction that also computes the
+//            BiCGSTAB scalars on the device).
+// Reference: AProductCore::Aproduct (src/AProductCore.cpp:461-515) with the
+// element-wise kernels of src/Kernel.cu:44-125, plus DDAModel::Aproductwithalb
+// (src/DDAModel.cpp:1194-1203) and DDAModel::bicgstab (src/DDAModel.cpp:899-1009).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "fft_smem.cuh"
+#include "operator.cuh"
+
+namespace tdda {
+
+constexpr int NT = 512;          // threads per CTA of the convolution passes
+constexpr int MAXI = 2;          // FFT work items a thread holds per stage
+constexpr int SMEM_MAX = 200 * 1024;
+constexpr int UPD_BLOCKS = 296;  // 2 x 148 SMs for the element-wise update
+
+// ----------------------------------------------------------------------------
+// deterministic reductions
+// ----------------------------------------------------------------------------
+template <int NQ> __device__ __forceinline__ void block_sum(double2 (&v)[NQ]) {
+    __shared__ double2 red[NQ > 0 ? NQ : 1][32];
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < NQ; ++q)
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            v[q].x += __shfl_xor_sync(0xffffffffu, v[q].x, off);
+            v[q].y += __shfl_xor_sync(0xffffffffu, v[q].y, off);
+        }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    if (lane == 0)
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) red[q][wid] = v[q];
+    __syncthreads();
+    if (wid == 0) {
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) {
+            v[q] = lane < nw ? red[q][lane] : make_double2(0.0, 0.0);
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                v[q].x += __shfl_xor_sync(0xffffffffu, v[q].x, off);
+                v[q].y += __shfl_xor_sync(0xffffffffu, v[q].y, off);
+            }
+        }
+    }
+}
+
+// Every block contributes NQ complex sums; the last block to finish adds the
+// per-block partials in block order and calls fin(rhs, totals) on thread 0.
+template <int NQ, class Fin>
+__device__ __forceinline__ void reduce_finalize(double2 (&v)[NQ], double2 *part, unsigned *counter,
+                                                int bid, int nblk, const Fin &fin, int rhs) {
+    block_sum<NQ>(v);
+    __shared__ int am_last;
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) part[(size_t)bid * NQ + q] = v[q];
+        __threadfence();
+        unsigned prev = atomicAdd(counter, 1u);
+        am_last = (prev == (unsigned)nblk - 1u);
+    }
+    __syncthreads();
+    if (!am_last) return;
+    __threadfence();
+    double2 s[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) s[q] = make_double2(0.0, 0.0);
+    for (int b = threadIdx.x; b < nblk; b += blockDim.x)
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) {
+            double2 w = __ldcg(part + (size_t)b * NQ + q);
+            s[q].x += w.x;
+            s[q].y += w.y;
+        }
+    block_sum<NQ>(s);
+    if (threadIdx.x == 0) {
+        fin(rhs, s);
+        *counter = 0u;
+    }
+}
+
+__device__ __forceinline__ bool dzero(double2 a) { return a.x == 0.0 && a.y == 0.0; }
+__device__ __forceinline__ bool dfinite(double2 a) { return isfinite(a.x) && isfinite(a.y); }
+
+// ----------------------------------------------------------------------------
+// the three passes
+// ----------------------------------------------------------------------------
+template <typename C, class Pro>
+__global__ void __launch_bounds__(NT) k_fwd_zy(ConvGeom g, C *__restrict__ T, const C *__restrict__ tw,
+                                               Pro pro) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *A = reinterpret_cast<C *>(smem_raw);
+    C *B = A + (size_t)g.ny * g.pA;
+    const int x = blockIdx.x, c = blockIdx.y, rhs = blockIdx.z;
+    if (pro.skip(rhs)) return;
+    const int nyz = g.ny * g.nz;
+    const long long cell0 = (long long)x * nyz;
+    for (int e = threadIdx.x; e < nyz; e += NT) {
+        int y = e / g.nz, z = e - y * g.nz;
+        A[y * g.pA + z] = pro.load(rhs, c, cell0 + e);
+    }
+    const int zpad = g.Lz - g.nz;
+    for (int e = threadIdx.x; e < g.ny * zpad; e += NT) {
+        int y = e / zpad, z = g.nz + (e - y * zpad);
+        A[y * g.pA + z] = czero<C>();
+    }
+    __syncthreads();
+    fft_smem<-1, MAXI>(A, g.Lz, g.ny, 1, g.pA, tw, g.Lmax);
+    C *Tc = T + ((size_t)(rhs * 3 + c) * g.nx + x) * (size_t)g.Ly * g.Lz;
+    for (int kz0 = 0; kz0 < g.Lz; kz0 += g.CK) {
+        for (int e = threadIdx.x; e < g.ny * g.CK; e += NT) {
+            int y = e / g.CK, kl = e - y * g.CK;
+            B[y * g.pB + kl] = A[y * g.pA + kz0 + kl];
+        }
+        for (int e = threadIdx.x; e < (g.Ly - g.ny) * g.CK; e += NT) {
+            int yy = e / g.CK, kl = e - yy * g.CK;
+            B[(g.ny + yy) * g.pB + kl] = czero<C>();
+        }
+        __syncthreads();
+        fft_smem<-1, MAXI>(B, g.Ly, g.CK, g.pB, 1, tw, g.Lmax);
+        for (int e = threadIdx.x; e < g.Ly * g.CK; e += NT) {
+            int ky = e / g.CK, kl = e - ky * g.CK;
+            Tc[(size_t)ky * g.Lz + kz0 + kl] = B[ky * g.pB + kl];
+        }
+        __syncthreads();
+    }
+}
+
+__device__ __forceinline__ void fold(int k, int L, int &fk, int &sgn) {
+    if (2 * k <= L) { fk = k; sgn = 1; }
+    else { fk = L - k; sgn = -1; }
+}
+
+template <typename C>
+__global__ void __launch_bounds__(NT) k_xconv(ConvGeom g, C *__restrict__ T, const C *__restrict__ ahat,
+                                              const C *__restrict__ tw, int nrhs,
+                                              const SolverState *__restrict__ st) {
+    using R = typename RealOf<C>::type;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *Cb = reinterpret_cast<C *>(smem_raw);
+    if (st != nullptr) {
+        bool any = false;
+        for (int r = 0; r < nrhs; ++r) any |= (st[r].done == 0);
+        if (!any) return;
+    }
+    const int ky = blockIdx.x, kz0 = blockIdx.y * g.CKx;
+    const int CKx = g.CKx, nbat = nrhs * 3 * CKx, pC = g.pC;
+    const size_t plane = (size_t)g.Ly * g.Lz;
+    const size_t off = (size_t)ky * g.Lz + kz0;
+    for (int e = threadIdx.x; e < g.nx * nbat; e += NT) {
+        int x = e / nbat, rem = e - x * nbat;
+        int rc = rem / CKx, kl = rem - rc * CKx;
+        Cb[x * pC + rem] = T[((size_t)rc * g.nx + x) * plane + off + kl];
+    }
+    for (int e = threadIdx.x; e < (g.Lx - g.nx) * nbat; e += NT) {
+        int xx = e / nbat, rem = e - xx * nbat;
+        Cb[(g.nx + xx) * pC + rem] = czero<C>();
+    }
+    __syncthreads();
+    fft_smem<-1, MAXI>(Cb, g.Lx, nbat, pC, 1, tw, g.Lmax);
+    int fky, sy;
+    fold(ky, g.Ly, fky, sy);
+    for (int e = threadIdx.x; e < g.Lx * CKx; e += NT) {
+        int kx = e / CKx, kl = e - kx * CKx;
+        int fkx, sx, fkz, sz;
+        fold(kx, g.Lx, fkx, sx);
+        fold(kz0 + kl, g.Lz, fkz, sz);
+        const C *a = ahat + (((size_t)fky * g.hx + fkx) * g.hz + fkz) * 6;
+        C axx = a[0], axy = (R)(sx * sy) * a[1], axz = (R)(sx * sz) * a[2];
+        C ayy = a[3], ayz = (R)(sy * sz) * a[4], azz = a[5];
+        C *v = Cb + kx * pC + kl;
+        for (int r = 0; r < nrhs; ++r) {
+            C *w = v + r * 3 * CKx;
+            C bx = w[0], by = w[CKx], bz = w[2 * CKx];
+            w[0] = axx * bx + axy * by + axz * bz;
+            w[CKx] = axy * bx + ayy * by + ayz * bz;
+            w[2 * CKx] = axz * bx + ayz * by + azz * bz;
+        }
+    }
+    __syncthreads();
+    fft_smem<+1, MAXI>(Cb, g.Lx, nbat, pC, 1, tw, g.Lmax);
+    for (int e = threadIdx.x; e < g.nx * nbat; e += NT) {
+        int x = e / nbat, rem = e - x * nbat;
+        int rc = rem / CKx, kl = rem - rc * CKx;
+        T[((size_t)rc * g.nx + x) * plane + off + kl] = Cb[x * pC + rem];
+    }
+}
+
+template <typename C, class Epi>
+__global__ void __launch_bounds__(NT) k_inv_yz(ConvGeom g, const C *__restrict__ T,
+                                               const C *__restrict__ tw, Epi epi) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *A = reinterpret_cast<C *>(smem_raw);
+    C *B = A + (size_t)g.ny * g.pA;
+    const int x = blockIdx.x, c = blockIdx.y, rhs = blockIdx.z;
+    if (epi.skip(rhs)) return;
+    const C *Tc = T + ((size_t)(rhs * 3 + c) * g.nx + x) * (size_t)g.Ly * g.Lz;
+    for (int kz0 = 0; kz0 < g.Lz; kz0 += g.CK) {
+        for (int e = threadIdx.x; e < g.Ly * g.CK; e += NT) {
+            int ky = e / g.CK, kl = e - ky * g.CK;
+            B[ky * g.pB + kl] = Tc[(size_t)ky * g.Lz + kz0 + kl];
+        }
+        __syncthreads();
+        fft_smem<+1, MAXI>(B, g.Ly, g.CK, g.pB, 1, tw, g.Lmax);
+        for (int e = threadIdx.x; e < g.ny * g.CK; e += NT) {
+            int y = e / g.CK, kl = e - y * g.CK;
+            A[y * g.pA + kz0 + kl] = B[y * g.pB + kl];
+        }
+        __syncthreads();
+    }
+    fft_smem<+1, MAXI>(A, g.Lz, g.ny, 1, g.pA, tw, g.Lmax);
+    const int nyz = g.ny * g.nz;
+    const long long cell0 = (long long)x * nyz;
+    double2 acc[Epi::NQ > 0 ? Epi::NQ : 1];
+#pragma unroll
+    for (int q = 0; q < (Epi::NQ > 0 ? Epi::NQ : 1); ++q) acc[q] = make_double2(0.0, 0.0);
+    for (int e = threadIdx.x; e < nyz; e += NT) {
+        int y = e / g.nz, z = e - y * g.nz;
+        epi.apply(rhs, c, cell0 + e, A[y * g.pA + z], acc);
+    }
+    if constexpr (Epi::NQ > 0) {
+        reduce_finalize<Epi::NQ>(acc, epi.part + (size_t)rhs * epi.pstride, epi.counter + rhs,
+                                 blockIdx.y * gridDim.x + blockIdx.x, gridDim.x * gridDim.y, epi, rhs);
+    }
+}
+
+// ----------------------------------------------------------------------------
+// prologues (what pass 1 transforms) and epilogues (what pass 3 produces)
+// ----------------------------------------------------------------------------
+template <typename C> struct VecBase {
+    long long nbox;
+    __device__ __forceinline__ size_t idx(int rhs, int c, long long cell) const {
+        return ((size_t)rhs * 3 + c) * (size_t)nbox + (size_t)cell;
+    }
+};
+
+template <typename C> struct ProLoad : VecBase<C> {
+    const C *x;
+    const SolverState *st;  // optional
+    __device__ bool skip(int rhs) const { return st != nullptr && st[rhs].done; }
+    __device__ C load(int rhs, int c, long long cell) const { return x[this->idx(rhs, c, cell)]; }
+};
+
+// p = r + beta (p - zeta Ap)   (first step: p = r)       src/DDAModel.cpp:929,972-973
+template <typename C> struct ProP : VecBase<C> {
+    const C *r;
+    C *p;
+    const C *Ap;
+    const SolverState *st;
+    int first;
+    __device__ bool skip(int rhs) const { return st[rhs].done; }
+    __device__ C load(int rhs, int c, long long cell) const {
+        size_t i = this->idx(rhs, c, cell);
+        C v = r[i];
+        if (!first) {
+            C beta = from_d<C>(st[rhs].beta), zeta = from_d<C>(st[rhs].zeta);
+            v = v + beta * (p[i] - zeta * Ap[i]);
+        }
+        p[i] = v;
+        return v;
+    }
+};
+
+// t = r - alpha Ap                                          src/DDAModel.cpp:933,976
+template <typename C> struct ProT : VecBase<C> {
+    const C *r;
+    const C *Ap;
+    C *t;
+    const SolverState *st;
+    __device__ bool skip(int rhs) const { return st[rhs].done; }
+    __device__ C load(int rhs, int c, long long cell) const {
+        size_t i = this->idx(rhs, c, cell);
+        C alpha = from_d<C>(st[rhs].alpha);
+        C v = r[i] - alpha * Ap[i];
+        t[i] = v;
+        return v;
+    }
+};
+
+template <typename C> struct EpiBase : VecBase<C> {
+    const unsigned char *mask;  // nullptr: every cell is a dipole
+    double2 *part;
+    unsigned *counter;
+    size_t pstride;
+    __device__ __forceinline__ C masked(long long cell, C conv) const {
+        if (mask != nullptr && mask[cell] == 0) return czero<C>();
+        return conv;
+    }
+};
+
+// y = conv (+ al o x)
+template <typename C> struct EpiMatvec : EpiBase<C> {
+    static constexpr int NQ = 0;
+    C *y;
+    const C *x;
+    const C *al;  // per cell, or nullptr
+    __device__ bool skip(int) const { return false; }
+    __device__ void apply(int rhs, int c, long long cell, C conv, double2 *) const {
+        size_t i = this->idx(rhs, c, cell);
+        C v = this->masked(cell, conv);
+        if (al != nullptr) v = v + al[cell] * x[i];
+        y[i] = v;
+    }
+    __device__ void operator()(int, const double2 *) const {}
+};
+
+// r = B - (A x0 + al o x0); r0 = r;  sums: r0.r, ||B||^2   src/DDAModel.cpp:925-928
+template <typename C> struct EpiInit : EpiBase<C> {
+    static constexpr int NQ = 2;
+    const C *x0, *b, *al;
+    C *r, *r0;
+    SolverState *st;
+    __device__ bool skip(int rhs) const { return false; }
+    __device__ void apply(int rhs, int c, long long cell, C conv, double2 *acc) const {
+        size_t i = this->idx(rhs, c, cell);
+        C ax = this->masked(cell, conv) + al[cell] * x0[i];
+        C bb = b[i];
+        C v = bb - ax;
+        r[i] = v;
+        r0[i] = v;
+        double2 vd = to_d(v), bd = to_d(bb);
+        double2 d = cdot1(vd, vd);
+        acc[0].x += d.x;
+        acc[0].y += d.y;
+        acc[1].x += bd.x * bd.x + bd.y * bd.y;
+    }
+    __device__ void operator()(int rhs, const double2 *s) const {
+        SolverState &S = st[rhs];
+        S.rho = s[0];
+        S.rho_prev = make_double2(0.0, 0.0);
+        S.enorm = sqrt(s[1].x);
+        S.err = S.enorm > 0 ? sqrt(s[0].x) / S.enorm : 0.0;
+        S.it = -1;
+        if (S.enorm == 0.0) {
+            S.done = 1;
+            S.status = TDDA_SOLVE_ZERO_RHS;
+            S.iters = 0;
+        }
+    }
+};
+
+// Ap = conv + al o p;  sum r0.Ap -> alpha = rho / (r0.Ap)    src/DDAModel.cpp:931-932,974-975
+template <typename C> struct EpiAp : EpiBase<C> {
+    static constexpr int NQ = 1;
+    const C *p, *al, *r0;
+    C *Ap;
+    SolverState *st;
+    __device__ bool skip(int rhs) const { return st[rhs].done; }
+    __device__ void apply(int rhs, int c, long long cell, C conv, double2 *acc) const {
+        size_t i = this->idx(rhs, c, cell);
+        C v = this->masked(cell, conv) + al[cell] * p[i];
+        Ap[i] = v;
+        double2 d = cdot1(to_d(r0[i]), to_d(v));
+        acc[0].x += d.x;
+        acc[0].y += d.y;
+    }
+    __device__ void operator()(int rhs, const double2 *s) const {
+        SolverState &S = st[rhs];
+        S.alpha = cdiv(S.rho, s[0]);
+    }
+};
+
+// At = conv + al o t;  sums At.t, At.At -> zeta              src/DDAModel.cpp:935-936,977-979
+template <typename C> struct EpiAt : EpiBase<C> {
+    static constexpr int NQ = 2;
+    const C *t, *al;
+    C *At;
+    SolverState *st;
+    __device__ bool skip(int rhs) const { return st[rhs].done; }
+    __device__ void apply(int rhs, int c, long long cell, C conv, double2 *acc) const {
+        size_t i = this->idx(rhs, c, cell);
+        C tv = t[i];
+        C v = this->masked(cell, conv) + al[cell] * tv;
+        At[i] = v;
+        double2 vd = to_d(v);
+        double2 d = cdot1(vd, to_d(tv));
+        acc[0].x += d.x;
+        acc[0].y += d.y;
+        double2 d2 = cdot1(vd, vd);
+        acc[1].x += d2.x;
+        acc[1].y += d2.y;
+    }
+    __device__ void operator()(int rhs, const double2 *s) const {
+        SolverState &S = st[rhs];
+        S.zeta = cdiv(s[0], s[1]);
+    }
+};
+
+// Finalize after the P/r update: bookkeeping of src/DDAModel.cpp:940-1008.
+struct FinUpdate {
+    SolverState *st;
+    __device__ void operator()(int rhs, const double2 *s) const {
+        SolverState &S = st[rhs];
+        S.rho_prev = S.rho;
+        S.rho = s[0];
+        S.err = sqrt(s[1].x) / S.enorm;
+        const int it = S.it;
+        if (it >= 0 && S.err <= S.tol) {
+            S.done = 1;
+            S.status = TDDA_SOLVE_CONVERGED;
+            S.iters = it + 1;
+        } else if (!isfinite(S.err)) {
+            S.done = 1;
+            S.status = TDDA_SOLVE_NONFINITE;
+            S.iters = it + 1;
+        } else if (it + 1 >= S.max_iter) {
+            S.done = 1;
+            S.status = TDDA_SOLVE_MAXITER;
+            S.iters = S.max_iter;
+        } else if (dzero(S.rho_prev)) {
+            S.done = 1;
+            S.status = TDDA_SOLVE_BREAKDOWN;
+            S.iters = it + 2;
+        } else {
+            // beta = (alpha / zeta) * (r0.r) / (r0.rl)
+            double2 az = cdiv(S.alpha, S.zeta);
+            double2 num = make_double2(az.x * S.rho.x - az.y * S.rho.y, az.x * S.rho.y + az.y * S.rho.x);
+            S.beta = cdiv(num, S.rho_prev);
+        }
+        S.it = it + 1;
+    }
+};
+
+// P += alpha p + zeta t;  r = t - zeta At;  sums r0.r, ||r||^2
+// (src/DDAModel.cpp:937-941,980-984, with alpha p + zeta r - alpha zeta Ap
+//  regrouped as alpha p + zeta t, which is the same vector since t = r - alpha Ap)
+template <typename C>
+__global__ void __launch_bounds__(NT) k_update(long long n, C *__restrict__ P, const C *__restrict__ p,
+                                               const C *__restrict__ t, const C *__restrict__ At,
+                                               C *__restrict__ r, const C *__restrict__ r0,
+                                               SolverState *st, double2 *part, unsigned *counter,
+                                               size_t pstride) {
+    const int rhs = blockIdx.y;
+    if (st[rhs].done) return;
+    const C alpha = from_d<C>(st[rhs].alpha), zeta = from_d<C>(st[rhs].zeta);
+    const size_t base = (size_t)rhs * n;
+    double2 acc[2] = {make_double2(0.0, 0.0), make_double2(0.0, 0.0)};
+    for (long long i = (long long)blockIdx.x * NT + threadIdx.x; i < n; i += (long long)gridDim.x * NT) {
+        size_t k = base + i;
+        C tv = t[k];
+        P[k] = P[k] + alpha * p[k] + zeta * tv;
+        C rn = tv - zeta * At[k];
+        r[k] = rn;
+        double2 rd = to_d(rn);
+        double2 d = cdot1(to_d(r0[k]), rd);
+        acc[0].x += d.x;
+        acc[0].y += d.y;
+        acc[1].x += rd.x * rd.x + rd.y * rd.y;
+    }
+    FinUpdate fin{st};
+    reduce_finalize<2>(acc, part + (size_t)rhs * pstride, counter + rhs, blockIdx.x, gridDim.x, fin, rhs);
+}
+
+// r = B, r0 = B, X = 0; sums r0.r, ||B||^2 (zero initial guess)
+template <typename C>
+__global__ void __launch_bounds__(NT) k_init_zero(long long n, const C *__restrict__ B, C *__restrict__ X,
+                                                  C *__restrict__ r, C *__restrict__ r0,
+                                                  SolverState *st, double2 *part, unsigned *counter,
+                                                  size_t pstride) {
+    const int rhs = blockIdx.y;
+    const size_t base = (size_t)rhs * n;
+    double2 acc[2] = {make_double2(0.0, 0.0), make_double2(0.0, 0.0)};
+    for (long long i = (long long)blockIdx.x * NT + threadIdx.x; i < n; i += (long long)gridDim.x * NT) {
+        size_t k = base + i;
+        C b = B[k];
+        r[k] = b;
+        r0[k] = b;
+        X[k] = czero<C>();
+        double2 bd = to_d(b);
+        double2 d = cdot1(bd, bd);
+        acc[0].x += d.x;
+        acc[0].y += d.y;
+        acc[1].x += bd.x * bd.x + bd.y * bd.y;
+    }
+    EpiInit<C> fin{};
+    fin.st = st;
+    reduce_finalize<2>(acc, part + (size_t)rhs * pstride, counter + rhs, blockIdx.x, gridDim.x, fin, rhs);
+}
+
+// ----------------------------------------------------------------------------
+// host side
+// ----------------------------------------------------------------------------
+static int gcd_i(int a, int b) { while (b) { int t = a % b; a = b; b = t; } return a; }
+static int lcm_i(int a, int b) { return a / gcd_i(a, b) * b; }
+
+int next_fft_len(int minlen) {
+    if (minlen <= 1) return 1;
+    int best = 1 << 30;
+    for (long long p2 = 1; p2 < (1LL << 30); p2 *= 2)
+        for (long long p3 = 1; p2 * p3 < (1LL << 30); p3 *= 3) {
+            long long v = p2 * p3;
+            if (v >= minlen && v < best) best = (int)v;
+        }
+    return best;
+}
+
+template <typename C> static void set_smem_attrs(int yz, int x) {
+    // the opt-in dynamic shared memory limit is a per-function attribute
+    cudaFuncSetAttribute(k_fwd_zy<C, ProLoad<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, yz);
+    cudaFuncSetAttribute(k_fwd_zy<C, ProP<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, yz);
+    cudaFuncSetAttribute(k_fwd_zy<C, ProT<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, yz);
+    cudaFuncSetAttribute(k_inv_yz<C, EpiMatvec<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, yz);
+    cudaFuncSetAttribute(k_inv_yz<C, EpiInit<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, yz);
+    cudaFuncSetAttribute(k_inv_yz<C, EpiAp<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, yz);
+    cudaFuncSetAttribute(k_inv_yz<C, EpiAt<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, yz);
+    cudaFuncSetAttribute(k_xconv<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, x);
+}
+
+static bool plan_geom(int nx, int ny, int nz, int nrhs, int esize, ConvGeom &g, std::string &why) {
+    g.nx = nx; g.ny = ny; g.nz = nz;
+    g.Lx = next_fft_len(2 * nx - 1);
+    g.Ly = next_fft_len(2 * ny - 1);
+    g.Lz = next_fft_len(2 * nz - 1);
+    g.hx = g.Lx / 2 + 1; g.hy = g.Ly / 2 + 1; g.hz = g.Lz / 2 + 1;
+    g.Lmax = lcm_i(lcm_i(g.Lx, g.Ly), g.Lz);
+    g.nbox = (long long)nx * ny * nz;
+    g.tcomp = (long long)nx * g.Ly * g.Lz;
+    g.nrhs = nrhs;
+    g.pA = (g.Lz % 2 == 0) ? g.Lz + 1 : g.Lz;
+    if (fft_max_items(g.Lz, ny, NT) > MAXI) { why = "ny too large for the z transform"; return false; }
+    g.CK = 0;
+    for (int ck = g.Lz; ck >= 1; --ck) {
+        if (g.Lz % ck) continue;
+        long long bytes = ((long long)ny * g.pA + (long long)g.Ly * ck) * esize;
+        if (bytes > SMEM_MAX) continue;
+        if (fft_max_items(g.Ly, ck, NT) > MAXI) continue;
+        g.CK = ck;
+        break;
+    }
+    if (g.CK == 0) { why = "slab does not fit in shared memory"; return false; }
+    g.pB = g.CK;
+    g.smem_yz = (int)(((long long)ny * g.pA + (long long)g.Ly * g.CK) * esize);
+    const int ckcap = esize == 16 ? 8 : 16;
+    g.CKx = 0;
+    for (int ck = std::min(g.Lz, ckcap); ck >= 1; --ck) {
+        if (g.Lz % ck) continue;
+        int nbat = nrhs * 3 * ck;
+        long long bytes = (long long)g.Lx * nbat * esize;
+        if (bytes > SMEM_MAX) continue;
+        if (fft_max_items(g.Lx, nbat, NT) > MAXI) continue;
+        g.CKx = ck;
+        break;
+    }
+    if (g.CKx == 0) { why = "x pencils do not fit in shared memory"; return false; }
+    g.pC = nrhs * 3 * g.CKx;
+    g.smem_x = g.Lx * g.pC * esize;
+    return true;
+}
+
+template <typename C> tdda_status ConvOperator<C>::init(int nx, int ny, int nz, int nrhs_cap_) {
+    nrhs_cap = nrhs_cap_;
+    set_smem_attrs<C>(SMEM_MAX, SMEM_MAX);
+    std::string why;
+    if (!plan_geom(nx, ny, nz, 1, (int)sizeof(C), g, why)) {
+        set_error("unsupported grid " + std::to_string(nx) + "x" + std::to_string(ny) + "x" +
+                  std::to_string(nz) + ": " + why);
+        return TDDA_ERR_UNSUPPORTED;
+    }
+    // twiddles in double, rounded once to C
+    std::vector<C> h(g.Lmax);
+    for (int j = 0; j < g.Lmax; ++j) {
+        long double ang = -2.0L * 3.141592653589793238462643383279502884L * (long double)j / g.Lmax;
+        h[j] = from_d<C>(make_double2((double)cosl(ang), (double)sinl(ang)));
+    }
+    TDDA_CUDA_TRY(cudaMalloc(&tw, sizeof(C) * g.Lmax));
+    TDDA_CUDA_TRY(cudaMemcpy(tw, h.data(), sizeof(C) * g.Lmax, cudaMemcpyHostToDevice));
+    TDDA_CUDA_TRY(cudaMalloc(&T, sizeof(C) * (size_t)nrhs_cap * 3 * g.tcomp));
+    partial_cap = std::max(3 * nx, UPD_BLOCKS) * 2;
+    TDDA_CUDA_TRY(cudaMalloc(&partials, sizeof(double2) * (size_t)partial_cap * nrhs_cap));
+    TDDA_CUDA_TRY(cudaMalloc(&counters, sizeof(unsigned) * (size_t)nrhs_cap));
+    TDDA_CUDA_TRY(cudaMemset(counters, 0, sizeof(unsigned) * (size_t)nrhs_cap));
+    return TDDA_OK;
+}
+
+template <typename C> void ConvOperator<C>::release() {
+    cudaFree(ahat); cudaFree(tw); cudaFree(T); cudaFree(partials); cudaFree(counters);
+    ahat = nullptr; tw = nullptr; T = nullptr; partials = nullptr; counters = nullptr;
+}
+
+template <typename C> static bool geom_for(const ConvOperator<C> &op, int nrhs, ConvGeom &g) {
+    std::string why;
+    if (nrhs == op.g.nrhs) { g = op.g; return true; }
+    return plan_geom(op.g.nx, op.g.ny, op.g.nz, nrhs, (int)sizeof(C), g, why);
+}
+
+template <typename C, class Pro, class Epi>
+static tdda_status run_conv(ConvOperator<C> &op, const ConvGeom &g, int nrhs, const Pro &pro,
+                            const Epi &epi, const SolverState *st, cudaStream_t s) {
+    dim3 g13(g.nx, 3, nrhs);
+    count_launches(1);
+    k_fwd_zy<C, Pro><<<g13, NT, g.smem_yz, s>>>(g, op.T, op.tw, pro);
+    dim3 g2(g.Ly, g.Lz / g.CKx, 1);
+    count_launches(1);
+    k_xconv<C><<<g2, NT, g.smem_x, s>>>(g, op.T, op.ahat, op.tw, nrhs, st);
+    count_launches(1);
+    k_inv_yz<C, Epi><<<g13, NT, g.smem_yz, s>>>(g, op.T, op.tw, epi);
+    return TDDA_OK;
+}
+
+template <typename C>
+tdda_status ConvOperator<C>::apply(const C *x, C *y, const C *al, int nrhs, cudaStream_t s) {
+    if (nrhs > nrhs_cap) { set_error("nrhs exceeds operator capacity"); return TDDA_ERR_BAD_ARG; }
+    ConvGeom gg;
+    if (!geom_for(*this, nrhs, gg)) { set_error("batch does not fit the x pass"); return TDDA_ERR_UNSUPPORTED; }
+    ProLoad<C> pro{};
+    pro.nbox = g.nbox; pro.x = x; pro.st = nullptr;
+    EpiMatvec<C> epi{};
+    epi.nbox = g.nbox; epi.mask = mask; epi.y = y; epi.x = x; epi.al = al;
+    run_conv(*this, gg, nrhs, pro, epi, nullptr, s);
+    TDDA_CUDA_TRY(cudaGetLastError());
+    return TDDA_OK;
+}
+
+template <typename C> tdda_status Krylov<C>::init(long long n3, int nrhs_) {
+    nrhs = nrhs_;
+    n = n3;
+    size_t bytes = sizeof(C) * (size_t)n * nrhs;
+    C **bufs[6] = {&r, &r0, &p, &t, &Ap, &At};
+    for (auto b : bufs) TDDA_CUDA_TRY(cudaMalloc(b, bytes));
+    TDDA_CUDA_TRY(cudaMalloc(&st, sizeof(SolverState) * nrhs));
+    TDDA_CUDA_TRY(cudaMallocHost(&st_host, sizeof(SolverState) * nrhs));
+    return TDDA_OK;
+}
+
+template <typename C> void Krylov<C>::release() {
+    C *bufs[6] = {r, r0, p, t, Ap, At};
+    for (auto b : bufs) cudaFree(b);
+    cudaFree(st);
+    cudaFreeHost(st_host);
+    r = r0 = p = t = Ap = At = nullptr;
+    st = nullptr;
+    st_host = nullptr;
+}
+
+template <typename C>
+tdda_status bicgstab_device(ConvOperator<C> &op, Krylov<C> &kv, const C *al, const C *B, C *X,
+                            int nrhs, bool x0_zero, int max_iter, double tol, cudaStream_t s,
+                            tdda_solve_info *info, const double *tols) {
+    if (nrhs > kv.nrhs || nrhs > op.nrhs_cap) { set_error("nrhs exceeds workspace"); return TDDA_ERR_BAD_ARG; }
+    ConvGeom g;
+    if (!geom_for(op, nrhs, g)) { set_error("batch does not fit the x pass"); return TDDA_ERR_UNSUPPORTED; }
+    const long long n = 3 * g.nbox;
+    for (int k = 0; k < nrhs; ++k) {
+        SolverState &S = kv.st_host[k];
+        std::memset(&S, 0, sizeof(S));
+        S.it = -1;
+        S.max_iter = max_iter;
+        S.tol = tols != nullptr ? tols[k] : tol;
+        S.status = TDDA_SOLVE_RUNNING;
+    }
+    TDDA_CUDA_TRY(cudaMemcpyAsync(kv.st, kv.st_host, sizeof(SolverState) * nrhs, cudaMemcpyHostToDevice, s));
+    const size_t ps = (size_t)op.partial_cap;
+    if (x0_zero) {
+        dim3 gi(UPD_BLOCKS, nrhs);
+        count_launches(1);
+        k_init_zero<C><<<gi, NT, 0, s>>>(n, B, X, kv.r, kv.r0, kv.st, op.partials, op.counters, ps);
+    } else {
+        ProLoad<C> pro{};
+        pro.nbox = g.nbox; pro.x = X; pro.st = nullptr;
+        EpiInit<C> epi{};
+        epi.nbox = g.nbox; epi.mask = op.mask; epi.part = op.partials; epi.counter = op.counters;
+        epi.pstride = ps; epi.x0 = X; epi.b = B; epi.al = al; epi.r = kv.r; epi.r0 = kv.r0; epi.st = kv.st;
+        run_conv(op, g, nrhs, pro, epi, nullptr, s);
+    }
+    TDDA_CUDA_TRY(cudaGetLastError());
+
+    // one BiCGSTAB step: Ap, alpha, t, At, zeta, P/r update, beta
+    auto step = [&](bool first) {
+        ProP<C> pp{};
+        pp.nbox = g.nbox; pp.r = kv.r; pp.p = kv.p; pp.Ap = kv.Ap; pp.st = kv.st; pp.first = first ? 1 : 0;
+        EpiAp<C> ea{};
+        ea.nbox = g.nbox; ea.mask = op.mask; ea.part = op.partials; ea.counter = op.counters; ea.pstride = ps;
+        ea.p = kv.p; ea.al = al; ea.r0 = kv.r0; ea.Ap = kv.Ap; ea.st = kv.st;
+        run_conv(op, g, nrhs, pp, ea, kv.st, s);
+        ProT<C> pt{};
+        pt.nbox = g.nbox; pt.r = kv.r; pt.Ap = kv.Ap; pt.t = kv.t; pt.st = kv.st;
+        EpiAt<C> et{};
+        et.nbox = g.nbox; et.mask = op.mask; et.part = op.partials; et.counter = op.counters; et.pstride = ps;
+        et.t = kv.t; et.al = al; et.At = kv.At; et.st = kv.st;
+        run_conv(op, g, nrhs, pt, et, kv.st, s);
+        dim3 gu(UPD_BLOCKS, nrhs);
+        count_launches(1);
+        k_update<C><<<gu, NT, 0, s>>>(n, X, kv.p, kv.t, kv.At, kv.r, kv.r0, kv.st, op.partials, op.counters, ps);
+    };
+
+    long long launched = 0;
+    bool first = true;
+    int chunk = 2;
+    for (;;) {
+        for (int k = 0; k < chunk; ++k) {
+            step(first);
+            first = false;
+        }
+        launched += chunk;
+        TDDA_CUDA_TRY(cudaGetLastError());
+        TDDA_CUDA_TRY(cudaMemcpyAsync(kv.st_host, kv.st, sizeof(SolverState) * nrhs, cudaMemcpyDeviceToHost, s));
+        TDDA_CUDA_TRY(cudaStreamSynchronize(s));
+        bool all = true;
+        for (int k = 0; k < nrhs; ++k) all &= (kv.st_host[k].done != 0);
+        if (all) break;
+        if (launched > (long long)max_iter + 64) {
+            set_error("solver did not report completion");
+            return TDDA_ERR_STATE;
+        }
+        chunk = std::min(chunk * 2, 16);
+    }
+    if (info != nullptr)
+        for (int k = 0; k < nrhs; ++k) {
+            const SolverState &S = kv.st_host[k];
+            info[k].iterations = S.iters;
+            info[k].error = S.err;
+            info[k].status = S.status;
+            info[k].refinements = 0;
+            info[k].inner_iterations = S.iters;
+            info[k].true_error = -1.0;
+        }
+    return TDDA_OK;
+}
+
+template struct ConvOperator<double2>;
+template struct ConvOperator<float2>;
+template struct Krylov<double2>;
+template struct Krylov<float2>;
+template tdda_status bicgstab_device<double2>(ConvOperator<double2> &, Krylov<double2> &, const double2 *,
+                                              const double2 *, double2 *, int, bool, int, double,
+                                              cudaStream_t, tdda_solve_info *, const double *);
+template tdda_status bicgstab_device<float2>(ConvOperator<float2> &, Krylov<float2> &, const float2 *,
+                                             const float2 *, float2 *, int, bool, int, double,
+                                             cudaStream_t, tdda_solve_info *, const double *);
+
+template <typename C>
+tdda_status profile_apply(ConvOperator<C> &op, const C *x, C *y, const C *al, int nrhs, int iters,
+                          cudaStream_t s, double *ms_total, double *ms_pass) {
+    ConvGeom g;
+    if (nrhs > op.nrhs_cap || !geom_for(op, nrhs, g)) { set_error("batch does not fit"); return TDDA_ERR_UNSUPPORTED; }
+    if (iters < 1) iters = 1;
+    ProLoad<C> pro{};
+    pro.nbox = g.nbox; pro.x = x; pro.st = nullptr;
+    EpiMatvec<C> epi{};
+    epi.nbox = g.nbox; epi.mask = op.mask; epi.y = y; epi.x = x; epi.al = al;
+    cudaEvent_t e0, e1;
+    TDDA_CUDA_TRY(cudaEventCreate(&e0));
+    TDDA_CUDA_TRY(cudaEventCreate(&e1));
+    dim3 g13(g.nx, 3, nrhs), g2(g.Ly, g.Lz / g.CKx, 1);
+    auto timed = [&](auto &&fn) -> double {
+        fn();  // warm
+        cudaEventRecord(e0, s);
+        for (int i = 0; i < iters; ++i) fn();
+        cudaEventRecord(e1, s);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        return (double)ms / iters;
+    };
+    *ms_total = timed([&] { run_conv(op, g, nrhs, pro, epi, nullptr, s); });
+    ms_pass[0] = timed([&] {
+        count_launches(1);
+        k_fwd_zy<C, ProLoad<C>><<<g13, NT, g.smem_yz, s>>>(g, op.T, op.tw, pro);
+    });
+    ms_pass[1] = timed([&] {
+        count_launches(1);
+        k_xconv<C><<<g2, NT, g.smem_x, s>>>(g, op.T, op.ahat, op.tw, nrhs, nullptr);
+    });
+    ms_pass[2] = timed([&] {
+        count_launches(1);
+        k_inv_yz<C, EpiMatvec<C>><<<g13, NT, g.smem_yz, s>>>(g, op.T, op.tw, epi);
+    });
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    TDDA_CUDA_TRY(cudaGetLastError());
+    return TDDA_OK;
+}
+
+template tdda_status profile_apply<double2>(ConvOperator<double2> &, const double2 *, double2 *, const double2 *,
+                                            int, int, cudaStream_t, double *, double *);
+template tdda_status profile_apply<float2>(ConvOperator<float2> &, const float2 *, float2 *, const float2 *, int,
+                                           int, cudaStream_t, double *, double *);
+
+tdda_status residual_c128(ConvOperator<double2> &op, const double2 *al, const double2 *B, const double2 *X,
+                          double2 *R, SolverState *st, int nrhs, cudaStream_t s) {
+    ConvGeom g;
+    if (nrhs > op.nrhs_cap || !geom_for(op, nrhs, g)) { set_error("batch does not fit"); return TDDA_ERR_UNSUPPORTED; }
+    ProLoad<double2> pro{};
+    pro.nbox = g.nbox; pro.x = X; pro.st = nullptr;
+    EpiInit<double2> epi{};
+    epi.nbox = g.nbox; epi.mask = op.mask; epi.part = op.partials; epi.counter = op.counters;
+    epi.pstride = (size_t)op.partial_cap; epi.x0 = X; epi.b = B; epi.al = al; epi.r = R; epi.r0 = R; epi.st = st;
+    run_conv(op, g, nrhs, pro, epi, nullptr, s);
+    TDDA_CUDA_TRY(cudaGetLastError());
+    return TDDA_OK;
+}
+
+}  // namespace tdda

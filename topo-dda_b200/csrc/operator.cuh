@@ -1,0 +1,75 @@
+// Host-side interface of the fused interaction operator and the BiCGSTAB
+// driver built on it.
+#pragma once
+
+#include "tdda_common.cuh"
+#include "../../include/tdda.h"
+
+namespace tdda {
+
+// Per right-hand side solver scalars, resident in device memory.
+struct SolverState {
+    double2 rho;        // r0 . r   (current r)
+    double2 rho_prev;   // r0 . rl  (previous r)
+    double2 alpha, zeta, beta;
+    double enorm;       // ||E||
+    double err;         // ||r|| / ||E|| (recursive residual)
+    int it;             // index of the next loop iteration (-1: pre-loop step pending)
+    int done;           // 1 once finished
+    int status;         // tdda_solve_status
+    int iters;          // loop passes executed, as the reference counts them
+    int max_iter;
+    double tol;
+};
+
+// Geometry + device buffers of one operator instance (one precision).
+template <typename C> struct ConvOperator {
+    ConvGeom g{};
+    C *ahat = nullptr;     // folded spectral tensor [hy][hx][hz][6], scaled by 1/(Lx Ly Lz)
+    C *tw = nullptr;       // twiddles exp(-2 pi i j / Lmax), j < Lmax
+    C *T = nullptr;        // spectral intermediate, nrhs_cap * 3 * tcomp
+    int nrhs_cap = 0;
+    double2 *partials = nullptr;  // reduction scratch
+    unsigned *counters = nullptr; // last-block counters
+    int partial_cap = 0;          // per rhs, per quantity
+    const unsigned char *mask = nullptr;  // cell -> in geometry (nullptr: full box)
+
+    tdda_status init(int nx, int ny, int nz, int nrhs_cap);
+    void release();
+    // y = A x (+ al o x when al != nullptr); x, y: [nrhs][3][nbox]
+    tdda_status apply(const C *x, C *y, const C *al, int nrhs, cudaStream_t s);
+};
+
+// Vectors of one BiCGSTAB instance ([nrhs][3][nbox] each) + states.
+template <typename C> struct Krylov {
+    int nrhs = 0;
+    long long n = 0;     // 3 * nbox
+    C *r = nullptr, *r0 = nullptr, *p = nullptr, *t = nullptr, *Ap = nullptr, *At = nullptr;
+    SolverState *st = nullptr;   // device
+    SolverState *st_host = nullptr;  // pinned mirror
+    tdda_status init(long long n3, int nrhs);
+    void release();
+};
+
+// BiCGSTAB of DDAModel::bicgstab on the fused operator: solves
+// (A + diag(al)) X = B for nrhs right-hand sides, X holds the initial guess
+// (nullptr-equivalent zero when x0_zero).  Runs fully on the device; the host
+// polls the done flags once per chunk of iterations.
+template <typename C>
+tdda_status bicgstab_device(ConvOperator<C> &op, Krylov<C> &kv, const C *al, const C *B, C *X,
+                            int nrhs, bool x0_zero, int max_iter, double tol, cudaStream_t s,
+                            tdda_solve_info *info, const double *tols /* per rhs, or nullptr */);
+
+// R = B - (A + diag al) X in complex128 (one fused convolution); st receives
+// enorm = ||B|| and err = ||R|| / ||B|| per right-hand side.
+tdda_status residual_c128(ConvOperator<double2> &op, const double2 *al, const double2 *B, const double2 *X,
+                          double2 *R, SolverState *st, int nrhs, cudaStream_t s);
+
+// Times `iters` back-to-back applications of the operator, then each pass
+// alone, with CUDA events on stream s: ms_total = mean per application,
+// ms_pass[0..2] = mean per launch of pass 1, 2, 3.
+template <typename C>
+tdda_status profile_apply(ConvOperator<C> &op, const C *x, C *y, const C *al, int nrhs, int iters,
+                          cudaStream_t s, double *ms_total, double *ms_pass);
+
+}  // namespace tdda

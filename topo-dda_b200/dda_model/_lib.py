@@ -1,0 +1,152 @@
+"""ctypes binding of libtdda.so (the C ABI declared in include/tdda.h).
+
+The library is built in tree next to this file (``python build_lib.py`` in the
+package root).  There is no fallback: importing the package without the
+library, or calling it on a machine without a CUDA device, raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libtdda.so")
+
+TDDA_OK = 0
+STATUS_NAMES = {
+    0: "ok", 1: "bad argument", 2: "out of device memory", 3: "not converged", 4: "breakdown",
+    5: "CUDA error", 6: "timeout", 7: "unsupported", 8: "invalid state",
+}
+SOLVE_STATUS = {0: "running", 1: "converged", 2: "max_iter", 3: "breakdown", 4: "nonfinite",
+                5: "zero_rhs"}
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int32)
+
+
+class Params(ctypes.Structure):
+    _fields_ = [
+        ("beta_min", ctypes.c_double), ("beta_max", ctypes.c_double), ("ita", ctypes.c_double),
+        ("beta_type", ctypes.c_char_p),
+        ("use_filter", ctypes.c_int),
+        ("symmetry_type", ctypes.c_char_p),
+        ("symmetry_axis", ctypes.c_double * 2),
+        ("is_periodic", ctypes.c_int),
+        ("objective_name", ctypes.c_char_p),
+        ("obj_para", _dp),
+        ("n_obj_para", ctypes.c_int),
+        ("num_x", ctypes.c_int), ("num_y", ctypes.c_int), ("num_z", ctypes.c_int),
+        ("num_total", ctypes.c_int),
+        ("n_K", ctypes.c_double * 3),
+        ("E0", ctypes.c_double),
+        ("n_E0", ctypes.c_double * 3),
+        ("lam", ctypes.c_double),
+        ("material", ctypes.c_double * 4),
+        ("nback", ctypes.c_double),
+        ("MAXm", ctypes.c_int), ("MAXn", ctypes.c_int),
+        ("Lm", ctypes.c_double), ("Ln", ctypes.c_double),
+        ("matrix_method", ctypes.c_char_p),
+        ("d", ctypes.c_double),
+        ("integral_delta", ctypes.c_double),
+        ("verbose", ctypes.c_int),
+        ("precision", ctypes.c_int),
+    ]
+
+
+class SolveInfo(ctypes.Structure):
+    _fields_ = [
+        ("iterations", ctypes.c_int),
+        ("error", ctypes.c_double),
+        ("status", ctypes.c_int),
+        ("refinements", ctypes.c_int),
+        ("inner_iterations", ctypes.c_int),
+        ("true_error", ctypes.c_double),
+    ]
+
+    def as_dict(self):
+        return {
+            "iterations": self.iterations, "error": self.error,
+            "status": SOLVE_STATUS.get(self.status, str(self.status)),
+            "refinements": self.refinements, "inner_iterations": self.inner_iterations,
+            "true_error": self.true_error,
+        }
+
+
+class ModelInfo(ctypes.Structure):
+    _fields_ = [
+        ("N", ctypes.c_int), ("NFpara", ctypes.c_int),
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+        ("Lx", ctypes.c_int), ("Ly", ctypes.c_int), ("Lz", ctypes.c_int),
+        ("K", ctypes.c_double),
+        ("material", ctypes.c_double * 4),
+        ("device_bytes", ctypes.c_longlong),
+        ("lattice_ms", ctypes.c_double), ("tensor_fft_ms", ctypes.c_double),
+    ]
+
+
+# every symbol include/tdda.h declares, with its ctypes signature
+SIGNATURES = {
+    "tdda_status_string": (ctypes.c_char_p, [ctypes.c_int]),
+    "tdda_last_error": (ctypes.c_char_p, []),
+    "tdda_abi_version": (ctypes.c_int, []),
+    "tdda_model_create": (ctypes.c_int, [ctypes.POINTER(Params), _ip, _dp, _dp, _dp, ctypes.c_int64,
+                                         ctypes.POINTER(ctypes.c_void_p)]),
+    "tdda_model_destroy": (None, [ctypes.c_void_p]),
+    "tdda_model_get_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ModelInfo)]),
+    "tdda_solve_electric_field": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_int, ctypes.c_double,
+                                                 ctypes.POINTER(SolveInfo)]),
+    "tdda_calculate_objective": (ctypes.c_int, [ctypes.c_void_p, _dp]),
+    "tdda_calculate_gradients": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_double,
+                                                ctypes.c_int, ctypes.c_double, _dp, ctypes.c_int64]),
+    "tdda_set_parameters": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_int64]),
+    "tdda_get_parameters": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_int64]),
+    "tdda_get_dielectrics": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_int64]),
+    "tdda_get_electric_field": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_int64]),
+    "tdda_get_polarization": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_int64]),
+    "tdda_matvec": (ctypes.c_int, [ctypes.c_void_p, _dp, _dp, ctypes.c_int]),
+    "tdda_solve_batch_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                               ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                               ctypes.c_void_p, ctypes.POINTER(SolveInfo)]),
+    "tdda_matvec_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                          ctypes.c_int, ctypes.c_int, ctypes.c_void_p]),
+    "tdda_set_densities": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_int64]),
+    "tdda_gradient_densities": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, _dp,
+                                               ctypes.c_int64, ctypes.POINTER(SolveInfo)]),
+    "tdda_profile_matvec": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                           _dp, _dp]),
+    "tdda_kernel_launches": (ctypes.c_longlong, []),
+    "tdda_set_precision": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+}
+
+_lib = None
+
+
+def load():
+    """Load libtdda.so once; raise if it is missing (no CPU fallback exists)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"libtdda.so not found at {LIB_PATH}: build the CUDA library first "
+                "(python topo-dda_b200/build_lib.py)")
+        lib = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+class TddaError(RuntimeError):
+    """A libtdda call failed; `.status` holds the tdda_status code."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+def check(status: int):
+    if status != TDDA_OK:
+        msg = load().tdda_last_error()
+        raise TddaError(status, msg.decode() if msg else "")
