@@ -38,7 +38,8 @@ typedef enum {
     TDDA_SOLVE_MAXITER = 2,     /* reference prints "does not converge" */
     TDDA_SOLVE_BREAKDOWN = 3,   /* r0 . rl == 0 (src/DDAModel.cpp:952-970) */
     TDDA_SOLVE_NONFINITE = 4,   /* residual became NaN/Inf */
-    TDDA_SOLVE_ZERO_RHS = 5     /* ||E|| == 0: solution is 0 */
+    TDDA_SOLVE_ZERO_RHS = 5,    /* ||E|| == 0: solution is 0 */
+    TDDA_SOLVE_STAGNATED = 6    /* mixed precision: residual stopped decreasing */
 } tdda_solve_status;
 
 typedef enum { TDDA_PREC_C128 = 0, TDDA_PREC_MIXED = 1 } tdda_precision;
@@ -163,6 +164,12 @@ long long tdda_kernel_launches(void);
 /* Solve precision of later solves: TDDA_PREC_C128, or TDDA_PREC_MIXED when
  * the model was created mixed (its complex64 operator exists). */
 tdda_status tdda_set_precision(tdda_model *m, int precision);
+/* Diagonal (Jacobi) scaling of later solves: 0 none -- the reference's plain
+ * BiCGSTAB, the default for complex128 models; 1 Jacobi -- the scaled system
+ * D^-1/2 A D^-1/2 (D = 1/alpha + the zero-offset lattice term) is solved
+ * inside a complex128 iterative refinement that stops on the true residual
+ * (the default for mixed-precision models). */
+tdda_status tdda_set_preconditioner(tdda_model *m, int kind);
 
 #ifdef __cplusplus
 }

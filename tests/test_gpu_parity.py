@@ -58,6 +58,21 @@ def test_matvec_matches_oracle(sici, shape, periodic, method):
     assert rel(dev.matvec(x, with_al=True), ora.aproduct_with_alb(x)) < 1e-12
 
 
+@pytest.mark.parametrize("shape,periodic", [((64, 64, 16), 1), ((128, 128, 32), 1), ((48, 40, 12), 0)])
+def test_matvec_large_grids(sici, shape, periodic):
+    """FFT lengths 128/256/96/80/24 (the benchmark grids), complex128 and complex64."""
+    from dda_model import DDAModel
+    from oracle.dda_oracle import OracleModel
+
+    nx, ny, nz = shape
+    kw = model_args(nx, ny, nz, sici, MAXm=periodic, MAXn=periodic, seed=17)
+    dev = DDAModel(**kw, precision="mixed")
+    ora = OracleModel(**kw)
+    x = _rand(3 * ora.N, 5)
+    ref = ora.aproduct_with_alb(x)
+    assert rel(dev.matvec(x), ref) < 1e-12
+
+
 def test_matvec_reference_fixture(fixture22, sici):
     """22x22x10, FCD, MAXm = MAXn = 50 (the reference's test structure)."""
     kw = fixture22_args(fixture22, sici)
@@ -196,6 +211,37 @@ def test_mixed_precision_reaches_complex128_accuracy(sici):
     assert res <= 1e-8
     ora.solveElectricField(P0, 10000, 1e-13)
     assert rel(P, ora.P) < 1e-6
+
+
+def test_mixed_precision_batched_rhs(sici):
+    """Several right-hand sides through one mixed-precision batched solve:
+    each meets the 1e-8 true residual and equals its single-RHS solve to the
+    solver tolerance."""
+    import torch
+
+    from dda_model import DDAModel
+    from oracle.dda_oracle import OracleModel
+
+    kw = model_args(12, 12, 6, sici, MAXm=2, MAXn=2, seed=13)
+    m = DDAModel(**kw, precision="mixed")
+    ora = OracleModel(**kw)
+    N3 = 3 * m.N
+    rng = np.random.default_rng(7)
+    B = rng.standard_normal((3, N3)) + 1j * rng.standard_normal((3, N3))
+    B[1] *= 1e3  # very different scales in one batch
+    Bt = torch.from_numpy(B).cuda()
+    Xt = torch.zeros_like(Bt)
+    s = torch.cuda.current_stream().cuda_stream
+    infos = m.solve_batch_device(Bt.data_ptr(), Xt.data_ptr(), 3, True, 10000, 1e-8, s)
+    torch.cuda.synchronize()
+    X = Xt.cpu().numpy()
+    for k in range(3):
+        assert infos[k]["status"] == "converged"
+        assert _true_res(ora, X[k], B[k]) <= 1e-8
+        xk = torch.zeros(N3, dtype=torch.complex128, device="cuda")
+        m.solve_batch_device(Bt[k].contiguous().data_ptr(), xk.data_ptr(), 1, True, 10000, 1e-8, s)
+        torch.cuda.synchronize()
+        assert rel(X[k], xk.cpu().numpy()) < 1e-7
 
 
 def test_nonbox_geometry(sici):

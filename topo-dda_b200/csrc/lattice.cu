@@ -279,7 +279,7 @@ static int pick_tile(int L, int want) {
 
 tdda_status build_tensor(const LatticeParams &P0, const double *si, const double *ci, long ntab,
                          double2 *ahat, float2 *ahat32, cudaStream_t s, double *lattice_ms,
-                         double *fft_ms) {
+                         double *fft_ms, double2 *a0) {
     LatticeParams P = P0;
     const size_t Lxyz = (size_t)P.Lx * P.Ly * P.Lz;
     double2 *G = nullptr, *sc = nullptr, *tw = nullptr;
@@ -335,6 +335,9 @@ tdda_status build_tensor(const LatticeParams &P0, const double *si, const double
     count_launches(1);
     k_lattice<<<(unsigned)((threads + LNT - 1) / LNT), LNT, 0, s>>>(P, G, lanes);
     cudaEventRecord(e1, s);
+    if (a0 != nullptr)
+        for (int l = 0; l < 6; ++l)
+            cudaMemcpyAsync(a0 + l, G + (size_t)l * Lxyz, sizeof(double2), cudaMemcpyDeviceToHost, s);
     // FFT along z (contiguous), y, x; the 6 components ride on grid.z
     {
         int TO = pick_tile(P.Lz, 16);

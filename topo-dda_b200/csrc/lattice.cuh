@@ -23,8 +23,10 @@ struct LatticeParams {
 
 // Lattice sums -> padded grid -> FP64 FFT -> folded spectral tensor
 // [hy][hx][hz][6] (scaled by 1/(Lx Ly Lz)); ahat32 optional complex64 copy.
+// a0 (optional, host double2[6]) receives the zero-offset tensor entry (the
+// sum over periodic images seen by every dipole itself).
 tdda_status build_tensor(const LatticeParams &P, const double *si, const double *ci, long ntab,
                          double2 *ahat, float2 *ahat32, cudaStream_t s, double *lattice_ms,
-                         double *fft_ms);
+                         double *fft_ms, double2 *a0);
 
 }  // namespace tdda

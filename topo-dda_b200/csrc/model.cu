@@ -213,24 +213,60 @@ __global__ void k_grad_mult(long long nbox, const double2 *__restrict__ lam, con
     }
 }
 
-// R32[k] = R[k] * scale[k]   (scale 0 parks a finished right-hand side)
-__global__ void k_to32_batch(long long n, int nrhs, const double2 *__restrict__ a, const double *__restrict__ scale,
-                             float2 *__restrict__ b) {
+// Rin[k] = sc o R[k] * scale[k] in the inner precision (scale 0 parks a
+// finished right-hand side; sc == nullptr: no Jacobi scaling)
+template <typename C>
+__global__ void k_to_inner(long long n, long long nbox, int nrhs, const double2 *__restrict__ a,
+                           const double *__restrict__ scale, const double2 *__restrict__ sc, C *__restrict__ b) {
     long long tot = n * nrhs;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < tot; i += (long long)gridDim.x * blockDim.x) {
         double s = scale[i / n];
-        b[i] = make_float2((float)(a[i].x * s), (float)(a[i].y * s));
+        double2 v = make_double2(a[i].x * s, a[i].y * s);
+        if (sc != nullptr) v = cmul_d(sc[(i % n) % nbox], v);
+        b[i] = from_d<C>(v);
     }
 }
 
-// X[k] += w[k] * D32[k]
-__global__ void k_axpy32_batch(long long n, int nrhs, const double *__restrict__ w, const float2 *__restrict__ d,
-                               double2 *__restrict__ x) {
+// X[k] += w[k] * sc o D[k]
+template <typename C>
+__global__ void k_axpy_inner(long long n, long long nbox, int nrhs, const double *__restrict__ w,
+                             const double2 *__restrict__ sc, const C *__restrict__ d, double2 *__restrict__ x) {
     long long tot = n * nrhs;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < tot; i += (long long)gridDim.x * blockDim.x) {
         double s = w[i / n];
-        x[i].x += s * (double)d[i].x;
-        x[i].y += s * (double)d[i].y;
+        double2 v = to_d(d[i]);
+        if (sc != nullptr) v = cmul_d(sc[(i % n) % nbox], v);
+        x[i].x += s * v.x;
+        x[i].y += s * v.y;
+    }
+}
+
+// principal square root
+__host__ __device__ inline double2 csqrt_d(double2 z) {
+    double r = hypot(z.x, z.y);
+    double re = sqrt(0.5 * (r + z.x));
+    double im = sqrt(0.5 * fmax(r - z.x, 0.0));
+    return make_double2(re, z.y < 0 ? -im : im);
+}
+
+// Jacobi scaling of the operator A + diag(al): D = al + a0 (a0: mean of the
+// diagonal of the zero-offset lattice entry), sc = D^(-1/2), alS = sc^2 al.
+__global__ void k_jacobi(long long nbox, const double2 *__restrict__ al, const unsigned char *__restrict__ mask,
+                         double2 a0, double2 *__restrict__ sc, double2 *__restrict__ alS,
+                         float2 *__restrict__ sc32, float2 *__restrict__ alS32) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nbox; i += (long long)gridDim.x * blockDim.x) {
+        double2 s = make_double2(1.0, 0.0), a = al[i];
+        if (mask == nullptr || mask[i] != 0) {
+            double2 d = make_double2(a.x + a0.x, a.y + a0.y);
+            s = cdiv(make_double2(1.0, 0.0), csqrt_d(d));
+        }
+        double2 as = cmul_d(cmul_d(s, s), a);
+        sc[i] = s;
+        alS[i] = as;
+        if (sc32 != nullptr) {
+            sc32[i] = make_float2((float)s.x, (float)s.y);
+            alS32[i] = make_float2((float)as.x, (float)as.y);
+        }
     }
 }
 
@@ -347,10 +383,17 @@ struct tdda_model {
     long long ext_cap = 0;
     double2 *bufB = nullptr, *bufX = nullptr;  // batch staging [nrhs][3][nbox]
     int buf_nrhs = 0;
-    // mixed precision workspace
+    // refinement workspace (mixed precision, or preconditioned complex128)
     double2 *Rm = nullptr;
     float2 *R32 = nullptr, *D32 = nullptr;
     int mixed_nrhs = 0;
+    double2 *R64 = nullptr, *D64 = nullptr;
+    int refine64_nrhs = 0, res_nrhs = 0;
+    // Jacobi scaling: 0 off (the reference's plain BiCGSTAB), 1 on
+    int precond = 0;
+    double2 a0{};                          // mean diagonal of the zero-offset tensor entry
+    double2 *sc64 = nullptr, *alS64 = nullptr;
+    float2 *sc32 = nullptr, *alS32 = nullptr;
     SolverState *st_res = nullptr, *st_res_host = nullptr;
     double *d_part = nullptr, *h_part = nullptr;
     // stats
@@ -362,7 +405,8 @@ struct tdda_model {
         op32.release();
         kv.release();
         kv32.release();
-        void *bufs[] = {d_cell, d_mask, d_rho, al, diel, al32, Einc, P, Eres, ext, bufB, bufX, Rm, R32, D32, st_res, d_part};
+        void *bufs[] = {d_cell, d_mask, d_rho, al,    diel,  al32, Einc, P,    Eres,  ext,   bufB, bufX,  Rm,
+                        R32,    D32,    st_res, d_part, R64, D64,  sc64, alS64, sc32, alS32};
         for (void *b : bufs) cudaFree(b);
         cudaFreeHost(st_res_host);
         cudaFreeHost(h_part);
@@ -438,6 +482,7 @@ static tdda_status ensure_krylov(tdda_model *m, int nrhs) {
 }
 
 static tdda_status ensure_mixed(tdda_model *m, int nrhs) {
+    TRY(ensure_op_cap(m, nrhs));  // the complex128 residual runs on the batch too
     if (m->kv32_nrhs < nrhs) {
         m->kv32.release();
         TRY(m->kv32.init(3 * m->nbox, nrhs));
@@ -460,19 +505,51 @@ static tdda_status ensure_mixed(tdda_model *m, int nrhs) {
         m->op32.nrhs_cap = nrhs;
     }
     if (m->mixed_nrhs < nrhs) {
-        cudaFree(m->Rm); cudaFree(m->R32); cudaFree(m->D32); cudaFree(m->st_res); cudaFreeHost(m->st_res_host);
-        m->Rm = nullptr; m->R32 = m->D32 = nullptr; m->st_res = nullptr; m->st_res_host = nullptr;
+        cudaFree(m->R32); cudaFree(m->D32);
+        m->R32 = m->D32 = nullptr;
         size_t n = 3 * (size_t)m->nbox * nrhs;
-        TDDA_CUDA_TRY(cudaMalloc(&m->Rm, sizeof(double2) * n));
         TDDA_CUDA_TRY(cudaMalloc(&m->R32, sizeof(float2) * n));
         TDDA_CUDA_TRY(cudaMalloc(&m->D32, sizeof(float2) * n));
-        TDDA_CUDA_TRY(cudaMemset(m->Rm, 0, sizeof(double2) * n));
         TDDA_CUDA_TRY(cudaMemset(m->R32, 0, sizeof(float2) * n));
         TDDA_CUDA_TRY(cudaMemset(m->D32, 0, sizeof(float2) * n));
-        TDDA_CUDA_TRY(cudaMalloc(&m->st_res, sizeof(SolverState) * nrhs));
-        TDDA_CUDA_TRY(cudaMallocHost(&m->st_res_host, sizeof(SolverState) * nrhs));
         m->mixed_nrhs = nrhs;
     }
+    return TDDA_OK;
+}
+
+// complex128 residual + per-RHS states shared by both refinement variants
+static tdda_status ensure_residual(tdda_model *m, int nrhs) {
+    static_assert(sizeof(SolverState) % 8 == 0, "SolverState layout");
+    TRY(ensure_op_cap(m, nrhs));
+    if (m->st_res != nullptr && m->res_nrhs >= nrhs) return TDDA_OK;
+    cudaFree(m->Rm); cudaFree(m->st_res); cudaFreeHost(m->st_res_host);
+    m->Rm = nullptr; m->st_res = nullptr; m->st_res_host = nullptr;
+    size_t n = 3 * (size_t)m->nbox * nrhs;
+    TDDA_CUDA_TRY(cudaMalloc(&m->Rm, sizeof(double2) * n));
+    TDDA_CUDA_TRY(cudaMemset(m->Rm, 0, sizeof(double2) * n));
+    TDDA_CUDA_TRY(cudaMalloc(&m->st_res, sizeof(SolverState) * nrhs));
+    TDDA_CUDA_TRY(cudaMallocHost(&m->st_res_host, sizeof(SolverState) * nrhs));
+    m->res_nrhs = nrhs;
+    return TDDA_OK;
+}
+
+static tdda_status ensure_refine(tdda_model *m, int nrhs, float2 *) {
+    TRY(ensure_residual(m, nrhs));
+    return ensure_mixed(m, nrhs);
+}
+
+static tdda_status ensure_refine(tdda_model *m, int nrhs, double2 *) {
+    TRY(ensure_residual(m, nrhs));
+    TRY(ensure_krylov(m, nrhs));
+    if (m->refine64_nrhs >= nrhs) return TDDA_OK;
+    cudaFree(m->R64); cudaFree(m->D64);
+    m->R64 = m->D64 = nullptr;
+    size_t n = 3 * (size_t)m->nbox * nrhs;
+    TDDA_CUDA_TRY(cudaMalloc(&m->R64, sizeof(double2) * n));
+    TDDA_CUDA_TRY(cudaMalloc(&m->D64, sizeof(double2) * n));
+    TDDA_CUDA_TRY(cudaMemset(m->R64, 0, sizeof(double2) * n));
+    TDDA_CUDA_TRY(cudaMemset(m->D64, 0, sizeof(double2) * n));
+    m->refine64_nrhs = nrhs;
     return TDDA_OK;
 }
 
@@ -488,6 +565,9 @@ static tdda_status update_alpha(tdda_model *m) {
     TDDA_CUDA_TRY(cudaMemcpyAsync(m->d_rho, rho.data(), sizeof(double) * m->nbox, cudaMemcpyHostToDevice, m->stream));
     count_launches(1);
     k_alpha<<<grid_for(m->nbox), 256, 0, m->stream>>>(m->nbox, m->d_rho, m->d_mask, m->ap, m->al, m->al32, m->diel);
+    count_launches(1);
+    k_jacobi<<<grid_for(m->nbox), 256, 0, m->stream>>>(m->nbox, m->al, m->d_mask, m->a0, m->sc64, m->alS64,
+                                                        m->sc32, m->alS32);
     TDDA_CUDA_TRY(cudaGetLastError());
     TDDA_CUDA_TRY(cudaStreamSynchronize(m->stream));
     return TDDA_OK;
@@ -497,20 +577,48 @@ static tdda_status solve_c128(tdda_model *m, const double2 *B, double2 *X, int n
                               int max_iter, double tol, tdda_solve_info *info) {
     TRY(ensure_krylov(m, nrhs));
     return bicgstab_device<double2>(m->op, m->kv, m->al, B, X, nrhs, x0_zero, max_iter, tol, m->stream, info,
-                                    nullptr);
+                                    nullptr, 0, nullptr);
 }
 
-// Mixed precision: complex64 BiCGSTAB on the normalised residual, complex128
-// residual and accumulation (iterative refinement) until ||B - A X||/||B|| <= tol.
-static tdda_status solve_mixed(tdda_model *m, const double2 *B, double2 *X, int nrhs, bool x0_zero,
-                               int max_iter, double tol, tdda_solve_info *info) {
-    TRY(ensure_mixed(m, nrhs));
+// Inner-solve workspace of the refinement driver, per inner precision.
+template <typename C> struct Inner {
+    ConvOperator<C> *op;
+    Krylov<C> *kv;
+    const C *al;  // al, or sc^2 al under Jacobi scaling
+    const C *sc;  // Jacobi scale or nullptr
+    C *R, *D;
+};
+
+static Inner<float2> inner_of(tdda_model *m, float2 *) {
+    const bool j = m->precond != 0;
+    return {&m->op32, &m->kv32, j ? m->alS32 : m->al32, j ? m->sc32 : nullptr, m->R32, m->D32};
+}
+
+static Inner<double2> inner_of(tdda_model *m, double2 *) {
+    const bool j = m->precond != 0;
+    return {&m->op, &m->kv, j ? m->alS64 : m->al, j ? m->sc64 : nullptr, m->R64, m->D64};
+}
+
+// Iterative refinement: the residual R = B - A X and the accumulation of X are
+// complex128; each correction solves A D = R / ||R|| with BiCGSTAB in the inner
+// precision C (complex64 for mixed precision), optionally Jacobi-scaled, until
+// the TRUE residual ||B - A X|| / ||B|| <= tol.
+template <typename C>
+static tdda_status solve_refined(tdda_model *m, const double2 *B, double2 *X, int nrhs, bool x0_zero,
+                                 int max_iter, double tol, tdda_solve_info *info) {
+    TRY(ensure_refine(m, nrhs, (C *)nullptr));
+    Inner<C> in = inner_of(m, (C *)nullptr);
+    const bool single = sizeof(C) == sizeof(float2);
     const long long n = 3 * m->nbox;
     if (x0_zero) TDDA_CUDA_TRY(cudaMemsetAsync(X, 0, sizeof(double2) * n * nrhs, m->stream));
     std::vector<int> done(nrhs, 0), refine(nrhs, 0), inner(nrhs, 0);
     std::vector<double> err(nrhs, 0.0);
-    std::vector<int> status(nrhs, TDDA_SOLVE_RUNNING);
+    std::vector<int> status(nrhs, TDDA_SOLVE_RUNNING), slow(nrhs, 0);
+    std::vector<double> prev(nrhs, 1e300);
     const int max_refine = 12;
+    // an inner complex64 solve that has not cut its residual by 10% in this many
+    // iterations has reached what single precision can give; refinement takes over
+    const int kInnerStall = 150;
     for (int outer = 0; outer <= max_refine; ++outer) {
         TRY(residual_c128(m->op, m->al, B, X, m->Rm, m->st_res, nrhs, m->stream));
         TDDA_CUDA_TRY(cudaMemcpyAsync(m->st_res_host, m->st_res, sizeof(SolverState) * nrhs, cudaMemcpyDeviceToHost, m->stream));
@@ -529,7 +637,12 @@ static tdda_status solve_mixed(tdda_model *m, const double2 *B, double2 *X, int 
                 done[k] = 1; status[k] = TDDA_SOLVE_NONFINITE;
             } else if (outer == max_refine || inner[k] >= max_iter) {
                 done[k] = 1; status[k] = TDDA_SOLVE_MAXITER;
+            } else {
+                // two refinements in a row that do not halve the true residual: stop
+                slow[k] = (S.err > 0.5 * prev[k]) ? slow[k] + 1 : 0;
+                if (slow[k] >= 2) { done[k] = 1; status[k] = TDDA_SOLVE_STAGNATED; }
             }
+            prev[k] = S.err;
             all &= (done[k] != 0);
         }
         if (all) break;
@@ -543,17 +656,20 @@ static tdda_status solve_mixed(tdda_model *m, const double2 *B, double2 *X, int 
             const double rn = S.err * S.enorm;
             h[k] = 1.0 / rn;                                   // scale into the inner RHS
             h[nrhs + k] = rn;                                  // scale of the correction
-            h[2 * nrhs + k] = std::max(0.5 * tol / S.err, 2e-6);  // inner tolerance
+            // inner tolerance: what this step must gain, floored where single
+            // precision stops paying off
+            h[2 * nrhs + k] = std::max(0.5 * tol / S.err, single ? 2e-6 : 0.0);
             budget = std::max(budget, max_iter - inner[k]);
         }
         TDDA_CUDA_TRY(cudaMemcpyAsync(m->d_part, h.data(), sizeof(double) * 3 * nrhs, cudaMemcpyHostToDevice, m->stream));
+        const double2 *sc = m->precond ? m->sc64 : nullptr;
         count_launches(1);
-        k_to32_batch<<<grid_for(n * nrhs), 256, 0, m->stream>>>(n, nrhs, m->Rm, m->d_part, m->R32);
+        k_to_inner<C><<<grid_for(n * nrhs), 256, 0, m->stream>>>(n, m->nbox, nrhs, m->Rm, m->d_part, sc, in.R);
         std::vector<tdda_solve_info> ii(nrhs);
-        TRY(bicgstab_device<float2>(m->op32, m->kv32, m->al32, m->R32, m->D32, nrhs, true, budget,
-                                    h[2 * nrhs], m->stream, ii.data(), h.data() + 2 * nrhs));
+        TRY(bicgstab_device<C>(*in.op, *in.kv, in.al, in.R, in.D, nrhs, true, budget, h[2 * nrhs], m->stream,
+                               ii.data(), h.data() + 2 * nrhs, kInnerStall, in.sc));
         count_launches(1);
-        k_axpy32_batch<<<grid_for(n * nrhs), 256, 0, m->stream>>>(n, nrhs, m->d_part + nrhs, m->D32, X);
+        k_axpy_inner<C><<<grid_for(n * nrhs), 256, 0, m->stream>>>(n, m->nbox, nrhs, m->d_part + nrhs, sc, in.D, X);
         TDDA_CUDA_TRY(cudaGetLastError());
         for (int k = 0; k < nrhs; ++k) {
             if (done[k]) continue;
@@ -577,7 +693,9 @@ static tdda_status solve_internal(tdda_model *m, const double2 *B, double2 *X, i
                                   int max_iter, double tol, tdda_solve_info *info) {
     if (max_iter < 0) return bad("max_iter must be >= 0");
     if (!(tol >= 0.0)) return bad("tolerance must be >= 0");
-    if (m->precision == TDDA_PREC_MIXED) return solve_mixed(m, B, X, nrhs, x0_zero, max_iter, tol, info);
+    if (m->precision == TDDA_PREC_MIXED)
+        return solve_refined<float2>(m, B, X, nrhs, x0_zero, max_iter, tol, info);
+    if (m->precond != 0) return solve_refined<double2>(m, B, X, nrhs, x0_zero, max_iter, tol, info);
     return solve_c128(m, B, X, nrhs, x0_zero, max_iter, tol, info);
 }
 
@@ -725,7 +843,14 @@ tdda_status tdda_model_create(const tdda_params *p, const int32_t *geometry, con
     TDDA_CUDA_TRY(cudaMemset(m->d_rho, 0, sizeof(double) * m->nbox));
     TDDA_CUDA_TRY(cudaMalloc(&m->al, sizeof(double2) * m->nbox));
     TDDA_CUDA_TRY(cudaMalloc(&m->diel, sizeof(double2) * m->nbox));
-    if (m->precision == TDDA_PREC_MIXED) TDDA_CUDA_TRY(cudaMalloc(&m->al32, sizeof(float2) * m->nbox));
+    TDDA_CUDA_TRY(cudaMalloc(&m->sc64, sizeof(double2) * m->nbox));
+    TDDA_CUDA_TRY(cudaMalloc(&m->alS64, sizeof(double2) * m->nbox));
+    if (m->precision == TDDA_PREC_MIXED) {
+        TDDA_CUDA_TRY(cudaMalloc(&m->al32, sizeof(float2) * m->nbox));
+        TDDA_CUDA_TRY(cudaMalloc(&m->sc32, sizeof(float2) * m->nbox));
+        TDDA_CUDA_TRY(cudaMalloc(&m->alS32, sizeof(float2) * m->nbox));
+        m->precond = 1;  // mixed precision refines Jacobi-scaled complex64 solves
+    }
     const size_t nvec = 3 * (size_t)m->nbox;
     TDDA_CUDA_TRY(cudaMalloc(&m->Einc, sizeof(double2) * nvec));
     TDDA_CUDA_TRY(cudaMalloc(&m->P, sizeof(double2) * nvec));
@@ -746,7 +871,9 @@ tdda_status tdda_model_create(const tdda_params *p, const int32_t *geometry, con
     std::vector<double> dummy(2, 0.0);
     const double *tsi = si ? si : dummy.data(), *tci = ci ? ci : dummy.data();
     long nt = (si && ci) ? (long)ntab : 2;
-    TRY(build_tensor(L, tsi, tci, nt, m->op.ahat, ahat32, m->stream, &m->lattice_ms, &m->fft_ms));
+    double2 a0[6];
+    TRY(build_tensor(L, tsi, tci, nt, m->op.ahat, ahat32, m->stream, &m->lattice_ms, &m->fft_ms, a0));
+    m->a0 = make_double2((a0[0].x + a0[3].x + a0[5].x) / 3.0, (a0[0].y + a0[3].y + a0[5].y) / 3.0);
 
     // incident field (src/DDAModel.cpp:312-316), internal layout
     {
@@ -1067,8 +1194,8 @@ tdda_status tdda_profile_matvec(tdda_model *m, int precision, int nrhs, int iter
         TRY(ensure_op_cap(m, nrhs));
         return profile_apply<double2>(m->op, m->bufB, m->bufX, m->al, nrhs, iters, m->stream, ms_matvec, ms_pass);
     }
-    if (m->precision != TDDA_PREC_MIXED) {
-        set_error("complex64 operator exists only in mixed-precision models");
+    if (m->op32.ahat == nullptr) {
+        set_error("complex64 operator exists only in models created mixed");
         return TDDA_ERR_UNSUPPORTED;
     }
     TRY(ensure_mixed(m, nrhs));
@@ -1089,6 +1216,13 @@ tdda_status tdda_set_precision(tdda_model *m, int precision) {
         return TDDA_OK;
     }
     return bad("precision must be 0 or 1");
+}
+
+tdda_status tdda_set_preconditioner(tdda_model *m, int kind) {
+    if (!m) return bad("null model");
+    if (kind != 0 && kind != 1) return bad("preconditioner must be 0 (none) or 1 (Jacobi)");
+    m->precond = kind;
+    return TDDA_OK;
 }
 
 }  // extern "C"

@@ -245,18 +245,26 @@ __global__ void __launch_bounds__(NT) k_inv_yz(ConvGeom g, const C *__restrict__
 // ----------------------------------------------------------------------------
 // prologues (what pass 1 transforms) and epilogues (what pass 3 produces)
 // ----------------------------------------------------------------------------
+// Optional diagonal (Jacobi) scaling: with sc = D^(-1/2) per cell the passes
+// apply S A S + diag(alS) (alS = sc^2 al) instead of A + diag(al): pass 1
+// scales what it transforms, pass 3 scales the convolution.  sc == nullptr is
+// the unscaled operator of the reference.
 template <typename C> struct VecBase {
     long long nbox;
+    const C *sc = nullptr;
     __device__ __forceinline__ size_t idx(int rhs, int c, long long cell) const {
         return ((size_t)rhs * 3 + c) * (size_t)nbox + (size_t)cell;
     }
+    __device__ __forceinline__ C scaled(long long cell, C v) const { return sc != nullptr ? sc[cell] * v : v; }
 };
 
 template <typename C> struct ProLoad : VecBase<C> {
     const C *x;
     const SolverState *st;  // optional
     __device__ bool skip(int rhs) const { return st != nullptr && st[rhs].done; }
-    __device__ C load(int rhs, int c, long long cell) const { return x[this->idx(rhs, c, cell)]; }
+    __device__ C load(int rhs, int c, long long cell) const {
+        return this->scaled(cell, x[this->idx(rhs, c, cell)]);
+    }
 };
 
 // p = r + beta (p - zeta Ap)   (first step: p = r)       src/DDAModel.cpp:929,972-973
@@ -275,7 +283,7 @@ template <typename C> struct ProP : VecBase<C> {
             v = v + beta * (p[i] - zeta * Ap[i]);
         }
         p[i] = v;
-        return v;
+        return this->scaled(cell, v);
     }
 };
 
@@ -291,7 +299,7 @@ template <typename C> struct ProT : VecBase<C> {
         C alpha = from_d<C>(st[rhs].alpha);
         C v = r[i] - alpha * Ap[i];
         t[i] = v;
-        return v;
+        return this->scaled(cell, v);
     }
 };
 
@@ -302,7 +310,7 @@ template <typename C> struct EpiBase : VecBase<C> {
     size_t pstride;
     __device__ __forceinline__ C masked(long long cell, C conv) const {
         if (mask != nullptr && mask[cell] == 0) return czero<C>();
-        return conv;
+        return this->scaled(cell, conv);
     }
 };
 
@@ -413,6 +421,10 @@ struct FinUpdate {
         S.rho = s[0];
         S.err = sqrt(s[1].x) / S.enorm;
         const int it = S.it;
+        if (S.stall_limit > 0 && it >= 0 && S.err < 0.9 * S.best_err) {
+            S.best_err = S.err;
+            S.best_it = it;
+        }
         if (it >= 0 && S.err <= S.tol) {
             S.done = 1;
             S.status = TDDA_SOLVE_CONVERGED;
@@ -425,6 +437,10 @@ struct FinUpdate {
             S.done = 1;
             S.status = TDDA_SOLVE_MAXITER;
             S.iters = S.max_iter;
+        } else if (S.stall_limit > 0 && it >= 0 && it - S.best_it >= S.stall_limit) {
+            S.done = 1;
+            S.status = TDDA_SOLVE_STAGNATED;
+            S.iters = it + 1;
         } else if (dzero(S.rho_prev)) {
             S.done = 1;
             S.status = TDDA_SOLVE_BREAKDOWN;
@@ -653,7 +669,7 @@ template <typename C> void Krylov<C>::release() {
 template <typename C>
 tdda_status bicgstab_device(ConvOperator<C> &op, Krylov<C> &kv, const C *al, const C *B, C *X,
                             int nrhs, bool x0_zero, int max_iter, double tol, cudaStream_t s,
-                            tdda_solve_info *info, const double *tols) {
+                            tdda_solve_info *info, const double *tols, int stall_limit, const C *sc) {
     if (nrhs > kv.nrhs || nrhs > op.nrhs_cap) { set_error("nrhs exceeds workspace"); return TDDA_ERR_BAD_ARG; }
     ConvGeom g;
     if (!geom_for(op, nrhs, g)) { set_error("batch does not fit the x pass"); return TDDA_ERR_UNSUPPORTED; }
@@ -664,6 +680,9 @@ tdda_status bicgstab_device(ConvOperator<C> &op, Krylov<C> &kv, const C *al, con
         S.it = -1;
         S.max_iter = max_iter;
         S.tol = tols != nullptr ? tols[k] : tol;
+        S.stall_limit = stall_limit;
+        S.best_it = 0;
+        S.best_err = 1e300;
         S.status = TDDA_SOLVE_RUNNING;
     }
     TDDA_CUDA_TRY(cudaMemcpyAsync(kv.st, kv.st_host, sizeof(SolverState) * nrhs, cudaMemcpyHostToDevice, s));
@@ -674,10 +693,11 @@ tdda_status bicgstab_device(ConvOperator<C> &op, Krylov<C> &kv, const C *al, con
         k_init_zero<C><<<gi, NT, 0, s>>>(n, B, X, kv.r, kv.r0, kv.st, op.partials, op.counters, ps);
     } else {
         ProLoad<C> pro{};
-        pro.nbox = g.nbox; pro.x = X; pro.st = nullptr;
+        pro.nbox = g.nbox; pro.x = X; pro.st = nullptr; pro.sc = sc;
         EpiInit<C> epi{};
         epi.nbox = g.nbox; epi.mask = op.mask; epi.part = op.partials; epi.counter = op.counters;
         epi.pstride = ps; epi.x0 = X; epi.b = B; epi.al = al; epi.r = kv.r; epi.r0 = kv.r0; epi.st = kv.st;
+        epi.sc = sc;
         run_conv(op, g, nrhs, pro, epi, nullptr, s);
     }
     TDDA_CUDA_TRY(cudaGetLastError());
@@ -689,12 +709,16 @@ tdda_status bicgstab_device(ConvOperator<C> &op, Krylov<C> &kv, const C *al, con
         EpiAp<C> ea{};
         ea.nbox = g.nbox; ea.mask = op.mask; ea.part = op.partials; ea.counter = op.counters; ea.pstride = ps;
         ea.p = kv.p; ea.al = al; ea.r0 = kv.r0; ea.Ap = kv.Ap; ea.st = kv.st;
+        pp.sc = sc;
+        ea.sc = sc;
         run_conv(op, g, nrhs, pp, ea, kv.st, s);
         ProT<C> pt{};
         pt.nbox = g.nbox; pt.r = kv.r; pt.Ap = kv.Ap; pt.t = kv.t; pt.st = kv.st;
         EpiAt<C> et{};
         et.nbox = g.nbox; et.mask = op.mask; et.part = op.partials; et.counter = op.counters; et.pstride = ps;
         et.t = kv.t; et.al = al; et.At = kv.At; et.st = kv.st;
+        pt.sc = sc;
+        et.sc = sc;
         run_conv(op, g, nrhs, pt, et, kv.st, s);
         dim3 gu(UPD_BLOCKS, nrhs);
         count_launches(1);
@@ -741,10 +765,12 @@ template struct Krylov<double2>;
 template struct Krylov<float2>;
 template tdda_status bicgstab_device<double2>(ConvOperator<double2> &, Krylov<double2> &, const double2 *,
                                               const double2 *, double2 *, int, bool, int, double,
-                                              cudaStream_t, tdda_solve_info *, const double *);
+                                              cudaStream_t, tdda_solve_info *, const double *, int,
+                                              const double2 *);
 template tdda_status bicgstab_device<float2>(ConvOperator<float2> &, Krylov<float2> &, const float2 *,
                                              const float2 *, float2 *, int, bool, int, double,
-                                             cudaStream_t, tdda_solve_info *, const double *);
+                                             cudaStream_t, tdda_solve_info *, const double *, int,
+                                             const float2 *);
 
 template <typename C>
 tdda_status profile_apply(ConvOperator<C> &op, const C *x, C *y, const C *al, int nrhs, int iters,

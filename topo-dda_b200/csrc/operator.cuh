@@ -20,6 +20,9 @@ struct SolverState {
     int iters;          // loop passes executed, as the reference counts them
     int max_iter;
     double tol;
+    int stall_limit;    // >0: stop when err has not dropped 10% in this many iterations
+    int best_it;
+    double best_err;
 };
 
 // Geometry + device buffers of one operator instance (one precision).
@@ -58,7 +61,9 @@ template <typename C> struct Krylov {
 template <typename C>
 tdda_status bicgstab_device(ConvOperator<C> &op, Krylov<C> &kv, const C *al, const C *B, C *X,
                             int nrhs, bool x0_zero, int max_iter, double tol, cudaStream_t s,
-                            tdda_solve_info *info, const double *tols /* per rhs, or nullptr */);
+                            tdda_solve_info *info, const double *tols /* per rhs, or nullptr */,
+                            int stall_limit /* 0: off (reference semantics) */,
+                            const C *sc /* Jacobi scale per cell (al must then be sc^2 al), or nullptr */);
 
 // R = B - (A + diag al) X in complex128 (one fused convolution); st receives
 // enorm = ||B|| and err = ||R|| / ||B|| per right-hand side.

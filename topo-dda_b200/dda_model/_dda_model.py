@@ -208,6 +208,12 @@ class DDAModel:
         """Switch later solves between "complex128" and "mixed" (mixed models only)."""
         _lib.check(self._lib.tdda_set_precision(self._handle, _PRECISIONS[precision]))
 
+    def setPreconditioner(self, kind):
+        """"none" (the reference's plain BiCGSTAB) or "jacobi" (diagonally scaled
+        solves inside a complex128 refinement on the true residual)."""
+        k = {"none": 0, "jacobi": 1}[kind]
+        _lib.check(self._lib.tdda_set_preconditioner(self._handle, k))
+
     @staticmethod
     def kernel_launches():
         return int(_lib.load().tdda_kernel_launches())

@@ -18,7 +18,7 @@ STATUS_NAMES = {
     5: "CUDA error", 6: "timeout", 7: "unsupported", 8: "invalid state",
 }
 SOLVE_STATUS = {0: "running", 1: "converged", 2: "max_iter", 3: "breakdown", 4: "nonfinite",
-                5: "zero_rhs"}
+                5: "zero_rhs", 6: "stagnated"}
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int32)
@@ -116,6 +116,7 @@ SIGNATURES = {
                                            _dp, _dp]),
     "tdda_kernel_launches": (ctypes.c_longlong, []),
     "tdda_set_precision": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "tdda_set_preconditioner": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
 }
 
 _lib = None
