@@ -171,6 +171,22 @@ tdda_status tdda_set_precision(tdda_model *m, int precision);
  * (the default for mixed-precision models). */
 tdda_status tdda_set_preconditioner(tdda_model *m, int kind);
 
+/* Allocation-free A.x (+ (1/alpha) o x when with_al != 0) for one vector.
+ * No counterpart in the reference.  For callers that must not have device
+ * memory allocated during a call -- a serving loop admitting work against a
+ * fixed device-memory budget, a host thread with a latency deadline (cudaMalloc
+ * and cudaFree may wait for the whole device), an application that plans every
+ * device byte up front.  x_dev, y_dev: complex128[3N] device arrays in dipole
+ * order; the work runs on `stream`.  The only extra memory is a fixed 32 MiB
+ * scratch array in the library image (held by every GPU that loads the library
+ * until exit): grids needing more (2 * 3 * nx*ny*nz * 16 B + 3 * nx*Ly*Lz * 16 B)
+ * are rejected with TDDA_ERR_BAD_ARG.  The first call on a device looks up the
+ * scratch's device address; make it before any stream capture begins.  Calls
+ * share the scratch: calls that overlap on the GPU race and must be serialised
+ * by the caller. */
+tdda_status tdda_matvec_device_noalloc(tdda_model *m, const void *x_dev, void *y_dev, int with_al,
+                                       void *stream);
+
 #ifdef __cplusplus
 }
 #endif

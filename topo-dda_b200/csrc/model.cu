@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "lattice.cuh"
+#include "model_view.cuh"
 #include "operator.cuh"
 
 namespace tdda {
@@ -413,6 +414,12 @@ struct tdda_model {
         if (stream) cudaStreamDestroy(stream);
     }
 };
+
+namespace tdda {
+ModelView model_view(const tdda_model *m) {
+    return {&m->op, m->al, m->d_cell, m->d_mask, (long long)m->N, m->nbox};
+}
+}  // namespace tdda
 
 #define TRY(x)                                \
     do {                                      \

@@ -645,6 +645,23 @@ tdda_status ConvOperator<C>::apply(const C *x, C *y, const C *al, int nrhs, cuda
     return TDDA_OK;
 }
 
+template <typename C>
+tdda_status apply_external_scratch(const ConvOperator<C> &op, C *T_ext, const C *x, C *y, const C *al,
+                                   cudaStream_t s) {
+    ConvOperator<C> view = op;  // same tensor, twiddles and plan; only the intermediate moves
+    view.T = T_ext;
+    ProLoad<C> pro{};
+    pro.nbox = op.g.nbox; pro.x = x; pro.st = nullptr;
+    EpiMatvec<C> epi{};
+    epi.nbox = op.g.nbox; epi.mask = op.mask; epi.y = y; epi.x = x; epi.al = al;
+    run_conv(view, op.g, 1, pro, epi, nullptr, s);
+    TDDA_CUDA_TRY(cudaGetLastError());
+    return TDDA_OK;
+}
+
+template tdda_status apply_external_scratch<double2>(const ConvOperator<double2> &, double2 *, const double2 *,
+                                                     double2 *, const double2 *, cudaStream_t);
+
 template <typename C> tdda_status Krylov<C>::init(long long n3, int nrhs_) {
     nrhs = nrhs_;
     n = n3;

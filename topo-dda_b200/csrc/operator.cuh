@@ -65,6 +65,12 @@ tdda_status bicgstab_device(ConvOperator<C> &op, Krylov<C> &kv, const C *al, con
                             int stall_limit /* 0: off (reference semantics) */,
                             const C *sc /* Jacobi scale per cell (al must then be sc^2 al), or nullptr */);
 
+// One operator application for one right-hand side whose spectral
+// intermediate lives in T_ext (3 * g.tcomp elements) instead of op.T.
+template <typename C>
+tdda_status apply_external_scratch(const ConvOperator<C> &op, C *T_ext, const C *x, C *y, const C *al,
+                                   cudaStream_t s);
+
 // R = B - (A + diag al) X in complex128 (one fused convolution); st receives
 // enorm = ||B|| and err = ||R|| / ||B|| per right-hand side.
 tdda_status residual_c128(ConvOperator<double2> &op, const double2 *al, const double2 *B, const double2 *X,

@@ -208,6 +208,14 @@ class DDAModel:
         """Switch later solves between "complex128" and "mixed" (mixed models only)."""
         _lib.check(self._lib.tdda_set_precision(self._handle, _PRECISIONS[precision]))
 
+    def matvec_device_noalloc(self, x_ptr, y_ptr, with_al=True, stream=None):
+        """A.x (+ (1/alpha) o x) on device buffers without any device allocation:
+        for callers that cannot have memory allocated during the call (fixed
+        memory budgets, latency-bound host threads).  Works in a fixed 32 MiB
+        scratch area of the library; larger grids raise.  Calls that overlap on
+        the GPU share that scratch and must be serialised by the caller."""
+        _lib.check(self._lib.tdda_matvec_device_noalloc(self._handle, x_ptr, y_ptr, 1 if with_al else 0, stream))
+
     def setPreconditioner(self, kind):
         """"none" (the reference's plain BiCGSTAB) or "jacobi" (diagonally scaled
         solves inside a complex128 refinement on the true residual)."""

@@ -117,6 +117,8 @@ SIGNATURES = {
     "tdda_kernel_launches": (ctypes.c_longlong, []),
     "tdda_set_precision": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "tdda_set_preconditioner": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "tdda_matvec_device_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                                  ctypes.c_int, ctypes.c_void_p]),
 }
 
 _lib = None
