@@ -61,6 +61,9 @@ def parse():
     ap.add_argument("--impl", default="tdda", choices=["tdda", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--small", action="store_true", help="32x32x8, M=5 (quick check, not a bench line)")
+    ap.add_argument("--profile-matvec", type=int, default=0, metavar="K",
+                    help="only build the benchmark model and apply the operator K times per precision "
+                         "(the case the kernel profiles capture); prints per-pass times")
     return ap.parse_args()
 
 
@@ -293,6 +296,11 @@ def main():
         f"{m.info['tensor_fft_ms']:.1f} ms)")
     rho = design(w)
     m.setDensities(rho)
+    if args.profile_matvec > 0:
+        for prec in ("mixed", "complex128"):
+            ms, passes = m.profile_matvec(prec, nrhs=1, iters=args.profile_matvec)
+            print(json.dumps({"precision": prec, "ms_matvec": ms, "ms_pass": passes}))
+        return 0
     N = m.N
     B = torch.from_numpy(np.stack([incident(w, 0), incident(w, 1)])).to(f"cuda:{local}")
     X = torch.zeros_like(B)

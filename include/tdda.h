@@ -131,6 +131,9 @@ tdda_status tdda_get_polarization(const tdda_model *m, double *out, int64_t n);
  * AProductCore::Aproduct (src/AProductCore.cpp:461-515) otherwise.
  * x, y: complex[3N] host arrays. */
 tdda_status tdda_matvec(tdda_model *m, const double *x, double *y, int with_al);
+/* The same product through the complex64 operator of a mixed-precision
+ * model (what its inner solves apply); x, y stay complex128 on the host. */
+tdda_status tdda_matvec_c64(tdda_model *m, const double *x, double *y, int with_al);
 
 /* Device-resident forms (pointers from cudaMalloc / torch; stream may be NULL).
  * Batched solve of (A + diag(1/alpha)) X_k = B_k for k < nrhs, complex[nrhs][3N]

@@ -58,7 +58,8 @@ def test_matvec_matches_oracle(sici, shape, periodic, method):
     assert rel(dev.matvec(x, with_al=True), ora.aproduct_with_alb(x)) < 1e-12
 
 
-@pytest.mark.parametrize("shape,periodic", [((64, 64, 16), 1), ((128, 128, 32), 1), ((48, 40, 12), 0)])
+@pytest.mark.parametrize("shape,periodic", [((64, 64, 16), 1), ((128, 128, 32), 1), ((48, 40, 12), 0),
+                                            ((16, 16, 8), 2), ((32, 32, 8), 0)])
 def test_matvec_large_grids(sici, shape, periodic):
     """FFT lengths 128/256/96/80/24 (the benchmark grids), complex128 and complex64."""
     from dda_model import DDAModel
@@ -71,6 +72,9 @@ def test_matvec_large_grids(sici, shape, periodic):
     x = _rand(3 * ora.N, 5)
     ref = ora.aproduct_with_alb(x)
     assert rel(dev.matvec(x), ref) < 1e-12
+    # single-precision operator of the mixed solver (FP32 FFTs): ~1e-6
+    assert rel(dev.matvec(x, precision="complex64"), ref) < 2e-6
+    assert rel(dev.matvec(x, with_al=False, precision="complex64"), ora.aproduct(x)) < 2e-6
 
 
 def test_matvec_reference_fixture(fixture22, sici):
@@ -242,6 +246,34 @@ def test_mixed_precision_batched_rhs(sici):
         m.solve_batch_device(Bt[k].contiguous().data_ptr(), xk.data_ptr(), 1, True, 10000, 1e-8, s)
         torch.cuda.synchronize()
         assert rel(X[k], xk.cpu().numpy()) < 1e-7
+
+
+@pytest.mark.parametrize("shape,nrhs", [((16, 16, 8), 2), ((16, 16, 8), 3), ((32, 32, 16), 2), ((64, 64, 16), 2),
+                                        ((128, 128, 32), 1)])
+@pytest.mark.parametrize("precision", ["complex128", "mixed"])
+def test_batched_rhs_on_compile_time_kernels(sici, shape, nrhs, precision):
+    """Batches on grids whose FFT lengths use the compile-time kernels."""
+    import torch
+
+    from dda_model import DDAModel
+    from oracle.dda_oracle import OracleModel
+
+    kw = model_args(*shape, sici, seed=19)
+    m = DDAModel(**kw, precision="mixed")
+    m.setPrecision(precision)
+    m.setPreconditioner("jacobi")
+    ora = OracleModel(**kw)
+    rng = np.random.default_rng(3)
+    B = rng.standard_normal((nrhs, 3 * m.N)) + 1j * rng.standard_normal((nrhs, 3 * m.N))
+    Bt = torch.from_numpy(B).cuda()
+    Xt = torch.zeros_like(Bt)
+    infos = m.solve_batch_device(Bt.data_ptr(), Xt.data_ptr(), nrhs, True, 10000, 1e-8,
+                                 torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    X = Xt.cpu().numpy()
+    for k in range(nrhs):
+        assert infos[k]["status"] == "converged", infos[k]
+        assert _true_res(ora, X[k], B[k]) <= 1e-8
 
 
 def test_nonbox_geometry(sici):

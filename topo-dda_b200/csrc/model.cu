@@ -1090,6 +1090,28 @@ tdda_status tdda_matvec(tdda_model *m, const double *x, double *y, int with_al) 
     return to_host(m, m->bufX, y, 1);
 }
 
+tdda_status tdda_matvec_c64(tdda_model *m, const double *x, double *y, int with_al) {
+    if (!m || !x || !y) return bad("null argument");
+    if (m->op32.ahat == nullptr) {
+        set_error("complex64 operator exists only in models created mixed");
+        return TDDA_ERR_UNSUPPORTED;
+    }
+    TRY(ensure_batch(m, 1));
+    TRY(ensure_mixed(m, 1));
+    const long long n = 3 * m->nbox;
+    TRY(to_internal(m, x, m->bufB, 1));
+    const double one = 1.0;
+    TDDA_CUDA_TRY(cudaMemcpyAsync(m->d_part, &one, sizeof(double), cudaMemcpyHostToDevice, m->stream));
+    count_launches(1);
+    k_to_inner<float2><<<grid_for(n), 256, 0, m->stream>>>(n, m->nbox, 1, m->bufB, m->d_part, nullptr, m->R32);
+    TRY(m->op32.apply(m->R32, m->D32, with_al ? m->al32 : nullptr, 1, m->stream));
+    TDDA_CUDA_TRY(cudaMemsetAsync(m->bufX, 0, sizeof(double2) * n, m->stream));
+    count_launches(1);
+    k_axpy_inner<float2><<<grid_for(n), 256, 0, m->stream>>>(n, m->nbox, 1, m->d_part, nullptr, m->D32, m->bufX);
+    TDDA_CUDA_TRY(cudaGetLastError());
+    return to_host(m, m->bufX, y, 1);
+}
+
 tdda_status tdda_solve_batch_device(tdda_model *m, const void *B_dev, void *X_dev, int nrhs, int x0_zero,
                                     int max_iter, double tol, void *stream, tdda_solve_info *infos) {
     if (!m || !X_dev || nrhs < 1) return bad("bad argument");

@@ -20,9 +20,10 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
-#include "fft_smem.cuh"
+#include "fft_fast.cuh"
 #include "operator.cuh"
 
 namespace tdda {
@@ -201,6 +202,176 @@ __global__ void __launch_bounds__(NT) k_xconv(ConvGeom g, C *__restrict__ T, con
         int x = e / nbat, rem = e - x * nbat;
         int rc = rem / CKx, kl = rem - rc * CKx;
         T[((size_t)rc * g.nx + x) * plane + off + kl] = Cb[x * pC + rem];
+    }
+}
+
+// Pass 2 for a compile-time x length L: same work as k_xconv, with the x
+// transforms on the ping-pong compile-time FFT (256-thread CTAs, several CTAs
+// per SM so one CTA's loads overlap another's transforms).
+constexpr int NT2 = 256;
+
+template <typename C, int L>
+__global__ void __launch_bounds__(NT2) k_xconv_fast(ConvGeom g, C *__restrict__ T, const C *__restrict__ ahat,
+                                                    const C *__restrict__ tw, int nrhs,
+                                                    const SolverState *__restrict__ st) {
+    using R = typename RealOf<C>::type;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    if (st != nullptr) {
+        bool any = false;
+        for (int r = 0; r < nrhs; ++r) any |= (st[r].done == 0);
+        if (!any) return;
+    }
+    const int CKx = g.CKx2, nbat = nrhs * 3 * CKx;
+    C *b0 = reinterpret_cast<C *>(smem_raw);
+    C *b1 = b0 + L * nbat;
+    const int ky = blockIdx.x, kz0 = blockIdx.y * CKx;
+    const size_t plane = (size_t)g.Ly * g.Lz;
+    const size_t off = (size_t)ky * g.Lz + kz0;
+    for (int e = threadIdx.x; e < g.nx * nbat; e += NT2) {
+        int x = e / nbat, rem = e - x * nbat;
+        int rc = rem / CKx, kl = rem - rc * CKx;
+        b0[x * nbat + rem] = T[((size_t)rc * g.nx + x) * plane + off + kl];
+    }
+    __syncthreads();
+    C *f = fft_fast<L, -1>(b0, b1, nbat, nbat, 1, tw, g.Lmax, g.nx, L);
+    int fky, sy;
+    fold(ky, g.Ly, fky, sy);
+    for (int e = threadIdx.x; e < L * CKx; e += NT2) {
+        int kx = e / CKx, kl = e - kx * CKx;
+        int fkx, sx, fkz, sz;
+        fold(kx, L, fkx, sx);
+        fold(kz0 + kl, g.Lz, fkz, sz);
+        const C *a = ahat + (((size_t)fky * g.hx + fkx) * g.hz + fkz) * 6;
+        C axx = a[0], axy = (R)(sx * sy) * a[1], axz = (R)(sx * sz) * a[2];
+        C ayy = a[3], ayz = (R)(sy * sz) * a[4], azz = a[5];
+        C *v = f + kx * nbat + kl;
+        for (int r = 0; r < nrhs; ++r) {
+            C *w = v + r * 3 * CKx;
+            C bx = w[0], by = w[CKx], bz = w[2 * CKx];
+            w[0] = axx * bx + axy * by + axz * bz;
+            w[CKx] = axy * bx + ayy * by + ayz * bz;
+            w[2 * CKx] = axz * bx + ayz * by + azz * bz;
+        }
+    }
+    __syncthreads();
+    C *res = fft_fast<L, +1>(f, f == b0 ? b1 : b0, nbat, nbat, 1, tw, g.Lmax, L, g.nx);
+    for (int e = threadIdx.x; e < g.nx * nbat; e += NT2) {
+        int x = e / nbat, rem = e - x * nbat;
+        int rc = rem / CKx, kl = rem - rc * CKx;
+        T[((size_t)rc * g.nx + x) * plane + off + kl] = res[x * nbat + rem];
+    }
+}
+
+template <typename C>
+static bool launch_xconv_fast(const ConvGeom &g, C *T, const C *ahat, const C *tw, int nrhs,
+                              const SolverState *st, cudaStream_t s) {
+    dim3 grid(g.Ly, g.Lz / g.CKx2, 1);
+    switch (g.Lx) {
+        case 256: k_xconv_fast<C, 256><<<grid, NT2, g.smem_x2, s>>>(g, T, ahat, tw, nrhs, st); return true;
+        case 128: k_xconv_fast<C, 128><<<grid, NT2, g.smem_x2, s>>>(g, T, ahat, tw, nrhs, st); return true;
+        case 64: k_xconv_fast<C, 64><<<grid, NT2, g.smem_x2, s>>>(g, T, ahat, tw, nrhs, st); return true;
+        case 32: k_xconv_fast<C, 32><<<grid, NT2, g.smem_x2, s>>>(g, T, ahat, tw, nrhs, st); return true;
+        default: return false;
+    }
+}
+
+static bool fast_x_length(int L) { return L == 256 || L == 128 || L == 64 || L == 32; }
+
+// Passes 1 and 3 for complex64 with compile-time (Lz, Ly): the whole padded
+// (x, component) slab [Ly][Lz + 1] sits in shared memory and 1024 threads
+// transform it in place, one butterfly each per stage; zero-padded inputs are
+// never stored (the first stage of each transform reads them as zero).
+constexpr int NT3 = 1024;
+constexpr int kSmemFast = 224 * 1024;  // dynamic SMEM opt-in of the slab kernels
+
+template <typename C, int LZ, int LY, class Pro>
+__global__ void __launch_bounds__(NT3, 1) k_fwd_zy_fast(ConvGeom g, C *__restrict__ T, const C *__restrict__ tw,
+                                                        Pro pro) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *S = reinterpret_cast<C *>(smem_raw);
+    constexpr int pS = LZ + 1;
+    const int x = blockIdx.x, c = blockIdx.y, rhs = blockIdx.z;
+    if (pro.skip(rhs)) return;
+    const int nyz = g.ny * g.nz;
+    const long long cell0 = (long long)x * nyz;
+    for (int e = threadIdx.x; e < nyz; e += NT3) {
+        int y = e / g.nz, z = e - y * g.nz;
+        S[y * pS + z] = pro.load(rhs, c, cell0 + e);
+    }
+    __syncthreads();
+    fft_ip<LZ, -1>(S, g.ny, 1, pS, tw, g.Lmax, g.nz);
+    fft_ip<LY, -1>(S, LZ, pS, 1, tw, g.Lmax, g.ny);
+    C *Tc = T + ((size_t)(rhs * 3 + c) * g.nx + x) * (size_t)(LY * LZ);
+    for (int e = threadIdx.x; e < LY * LZ; e += NT3) Tc[e] = S[(e / LZ) * pS + (e % LZ)];
+}
+
+template <typename C, int LZ, int LY, class Epi>
+__global__ void __launch_bounds__(NT3, 1) k_inv_yz_fast(ConvGeom g, const C *__restrict__ T,
+                                                        const C *__restrict__ tw, Epi epi) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *S = reinterpret_cast<C *>(smem_raw);
+    constexpr int pS = LZ + 1;
+    const int x = blockIdx.x, c = blockIdx.y, rhs = blockIdx.z;
+    if (epi.skip(rhs)) return;
+    const C *Tc = T + ((size_t)(rhs * 3 + c) * g.nx + x) * (size_t)(LY * LZ);
+    for (int e = threadIdx.x; e < LY * LZ; e += NT3) S[(e / LZ) * pS + (e % LZ)] = Tc[e];
+    __syncthreads();
+    fft_ip<LY, +1>(S, LZ, pS, 1, tw, g.Lmax, LY, g.ny);
+    fft_ip<LZ, +1>(S, g.ny, 1, pS, tw, g.Lmax, LZ, g.nz);
+    const int nyz = g.ny * g.nz;
+    const long long cell0 = (long long)x * nyz;
+    double2 acc[Epi::NQ > 0 ? Epi::NQ : 1];
+#pragma unroll
+    for (int q = 0; q < (Epi::NQ > 0 ? Epi::NQ : 1); ++q) acc[q] = make_double2(0.0, 0.0);
+    for (int e = threadIdx.x; e < nyz; e += NT3) {
+        int y = e / g.nz, z = e - y * g.nz;
+        epi.apply(rhs, c, cell0 + e, S[y * pS + z], acc);
+    }
+    if constexpr (Epi::NQ > 0) {
+        reduce_finalize<Epi::NQ>(acc, epi.part + (size_t)rhs * epi.pstride, epi.counter + rhs,
+                                 blockIdx.y * gridDim.x + blockIdx.x, gridDim.x * gridDim.y, epi, rhs);
+    }
+}
+
+// (Lz, Ly) pairs with a compile-time slab kernel
+#define TDDA_YZ_PAIRS(X) X(64, 256) X(32, 128) X(16, 64) X(16, 32)
+
+static bool fast_yz_pair(int Lz, int Ly) {
+#define TDDA_PAIR_TEST(a, b) if (Lz == a && Ly == b) return true;
+    TDDA_YZ_PAIRS(TDDA_PAIR_TEST)
+#undef TDDA_PAIR_TEST
+    return false;
+}
+
+template <typename C, class Pro>
+static bool launch_fwd_fast(const ConvGeom &g, dim3 grid, C *T, const C *tw, const Pro &pro, cudaStream_t s) {
+    if constexpr (!std::is_same<C, float2>::value) {
+        return false;
+    } else {
+#define TDDA_FWD_CASE(a, b)                                                                  \
+    if (g.Lz == a && g.Ly == b) {                                                            \
+        k_fwd_zy_fast<C, a, b, Pro><<<grid, NT3, g.smem_yz2, s>>>(g, T, tw, pro);           \
+        return true;                                                                         \
+    }
+        TDDA_YZ_PAIRS(TDDA_FWD_CASE)
+#undef TDDA_FWD_CASE
+        return false;
+    }
+}
+
+template <typename C, class Epi>
+static bool launch_inv_fast(const ConvGeom &g, dim3 grid, const C *T, const C *tw, const Epi &epi, cudaStream_t s) {
+    if constexpr (!std::is_same<C, float2>::value) {
+        return false;
+    } else {
+#define TDDA_INV_CASE(a, b)                                                                  \
+    if (g.Lz == a && g.Ly == b) {                                                            \
+        k_inv_yz_fast<C, a, b, Epi><<<grid, NT3, g.smem_yz2, s>>>(g, T, tw, epi);           \
+        return true;                                                                         \
+    }
+        TDDA_YZ_PAIRS(TDDA_INV_CASE)
+#undef TDDA_INV_CASE
+        return false;
     }
 }
 
@@ -538,6 +709,25 @@ template <typename C> static void set_smem_attrs(int yz, int x) {
     cudaFuncSetAttribute(k_inv_yz<C, EpiAp<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, yz);
     cudaFuncSetAttribute(k_inv_yz<C, EpiAt<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, yz);
     cudaFuncSetAttribute(k_xconv<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, x);
+    cudaFuncSetAttribute(k_xconv_fast<C, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, x);
+    cudaFuncSetAttribute(k_xconv_fast<C, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, x);
+    cudaFuncSetAttribute(k_xconv_fast<C, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, x);
+    cudaFuncSetAttribute(k_xconv_fast<C, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, x);
+    if constexpr (std::is_same<C, float2>::value) {
+        // dynamic + static shared memory must stay within the 227 KB opt-in limit;
+        // the epilogue kernels carry ~1 KB of static reduction scratch
+#define TDDA_ATTR(a, b)                                                                                            \
+    cudaFuncSetAttribute(k_fwd_zy_fast<C, a, b, ProLoad<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemFast);   \
+    cudaFuncSetAttribute(k_fwd_zy_fast<C, a, b, ProP<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemFast);      \
+    cudaFuncSetAttribute(k_fwd_zy_fast<C, a, b, ProT<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemFast);      \
+    cudaFuncSetAttribute(k_inv_yz_fast<C, a, b, EpiMatvec<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemFast); \
+    cudaFuncSetAttribute(k_inv_yz_fast<C, a, b, EpiInit<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemFast);   \
+    cudaFuncSetAttribute(k_inv_yz_fast<C, a, b, EpiAp<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemFast);     \
+    cudaFuncSetAttribute(k_inv_yz_fast<C, a, b, EpiAt<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemFast);
+        TDDA_YZ_PAIRS(TDDA_ATTR)
+#undef TDDA_ATTR
+    }
+    cudaGetLastError();  // a refused opt-in shows up at launch time, not here
 }
 
 static bool plan_geom(int nx, int ny, int nz, int nrhs, int esize, ConvGeom &g, std::string &why) {
@@ -578,6 +768,25 @@ static bool plan_geom(int nx, int ny, int nz, int nrhs, int esize, ConvGeom &g, 
     if (g.CKx == 0) { why = "x pencils do not fit in shared memory"; return false; }
     g.pC = nrhs * 3 * g.CKx;
     g.smem_x = g.Lx * g.pC * esize;
+    // compile-time slab kernels for passes 1 and 3 (complex64 only)
+    g.smem_yz2 = (int)((long long)g.Ly * (g.Lz + 1) * esize);
+    g.fast_yz = (esize == 8 && fast_yz_pair(g.Lz, g.Ly) && g.smem_yz2 <= kSmemFast &&
+                 ny * fast_max_items(g.Lz) <= NT3 && g.Lz * fast_max_items(g.Ly) <= NT3)
+                    ? 1
+                    : 0;
+    // compile-time-length pass 2: two ping-pong buffers, at most ~100 KB so
+    // that two CTAs share an SM; runs of >= 64 bytes along kz
+    g.fast_x = fast_x_length(g.Lx) ? 1 : 0;
+    g.CKx2 = 0;
+    for (int ck = std::min(g.Lz, esize == 16 ? 4 : 8); ck >= 1 && g.fast_x; --ck) {
+        if (g.Lz % ck) continue;
+        long long bytes = 2LL * g.Lx * nrhs * 3 * ck * esize;
+        if (bytes > 100 * 1024 && ck > 1) continue;
+        g.CKx2 = ck;
+        g.smem_x2 = (int)bytes;
+        break;
+    }
+    if (g.CKx2 == 0 || g.smem_x2 > SMEM_MAX) g.fast_x = 0;
     return true;
 }
 
@@ -622,12 +831,15 @@ static tdda_status run_conv(ConvOperator<C> &op, const ConvGeom &g, int nrhs, co
                             const Epi &epi, const SolverState *st, cudaStream_t s) {
     dim3 g13(g.nx, 3, nrhs);
     count_launches(1);
-    k_fwd_zy<C, Pro><<<g13, NT, g.smem_yz, s>>>(g, op.T, op.tw, pro);
+    if (!(g.fast_yz && launch_fwd_fast<C, Pro>(g, g13, op.T, op.tw, pro, s)))
+        k_fwd_zy<C, Pro><<<g13, NT, g.smem_yz, s>>>(g, op.T, op.tw, pro);
     dim3 g2(g.Ly, g.Lz / g.CKx, 1);
     count_launches(1);
-    k_xconv<C><<<g2, NT, g.smem_x, s>>>(g, op.T, op.ahat, op.tw, nrhs, st);
+    if (!(g.fast_x && launch_xconv_fast<C>(g, op.T, op.ahat, op.tw, nrhs, st, s)))
+        k_xconv<C><<<g2, NT, g.smem_x, s>>>(g, op.T, op.ahat, op.tw, nrhs, st);
     count_launches(1);
-    k_inv_yz<C, Epi><<<g13, NT, g.smem_yz, s>>>(g, op.T, op.tw, epi);
+    if (!(g.fast_yz && launch_inv_fast<C, Epi>(g, g13, op.T, op.tw, epi, s)))
+        k_inv_yz<C, Epi><<<g13, NT, g.smem_yz, s>>>(g, op.T, op.tw, epi);
     return TDDA_OK;
 }
 
@@ -816,15 +1028,18 @@ tdda_status profile_apply(ConvOperator<C> &op, const C *x, C *y, const C *al, in
     *ms_total = timed([&] { run_conv(op, g, nrhs, pro, epi, nullptr, s); });
     ms_pass[0] = timed([&] {
         count_launches(1);
-        k_fwd_zy<C, ProLoad<C>><<<g13, NT, g.smem_yz, s>>>(g, op.T, op.tw, pro);
+        if (!(g.fast_yz && launch_fwd_fast<C, ProLoad<C>>(g, g13, op.T, op.tw, pro, s)))
+            k_fwd_zy<C, ProLoad<C>><<<g13, NT, g.smem_yz, s>>>(g, op.T, op.tw, pro);
     });
     ms_pass[1] = timed([&] {
         count_launches(1);
-        k_xconv<C><<<g2, NT, g.smem_x, s>>>(g, op.T, op.ahat, op.tw, nrhs, nullptr);
+        if (!(g.fast_x && launch_xconv_fast<C>(g, op.T, op.ahat, op.tw, nrhs, nullptr, s)))
+            k_xconv<C><<<g2, NT, g.smem_x, s>>>(g, op.T, op.ahat, op.tw, nrhs, nullptr);
     });
     ms_pass[2] = timed([&] {
         count_launches(1);
-        k_inv_yz<C, EpiMatvec<C>><<<g13, NT, g.smem_yz, s>>>(g, op.T, op.tw, epi);
+        if (!(g.fast_yz && launch_inv_fast<C, EpiMatvec<C>>(g, g13, op.T, op.tw, epi, s)))
+            k_inv_yz<C, EpiMatvec<C>><<<g13, NT, g.smem_yz, s>>>(g, op.T, op.tw, epi);
     });
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);

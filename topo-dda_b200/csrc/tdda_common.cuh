@@ -90,6 +90,11 @@ struct ConvGeom {
     int pC;             // SMEM row pitch of the [kx][batch] buffer
     int smem_yz;        // dynamic SMEM bytes, passes 1 and 3
     int smem_x;         // dynamic SMEM bytes, pass 2
+    int fast_yz;        // 1: passes 1 and 3 use the compile-time (Lz, Ly) slab kernels
+    int smem_yz2;       // their dynamic SMEM bytes
+    int fast_x;         // 1: pass 2 uses the compile-time-length kernel for Lx
+    int CKx2;           // kz chunk of that kernel
+    int smem_x2;        // its dynamic SMEM bytes (two ping-pong buffers)
 };
 
 int next_fft_len(int minlen);   // smallest 2^a 3^b >= minlen

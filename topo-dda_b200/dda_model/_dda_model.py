@@ -160,12 +160,13 @@ class DDAModel:
         _lib.check(self._lib.tdda_get_polarization(self._handle, _dp(g.view(np.float64)), g.size))
         return g
 
-    def matvec(self, x, with_al=True):
-        """A.x (+ (1/alpha) o x): AProductCore::Aproduct / DDAModel::Aproductwithalb."""
+    def matvec(self, x, with_al=True, precision="complex128"):
+        """A.x (+ (1/alpha) o x): AProductCore::Aproduct / DDAModel::Aproductwithalb.
+        precision="complex64" applies the single-precision operator of a mixed model."""
         xx = _c128(x, 3 * self.N, "x")
         y = np.zeros_like(xx)
-        _lib.check(self._lib.tdda_matvec(self._handle, _dp(xx.view(np.float64)), _dp(y.view(np.float64)),
-                                         1 if with_al else 0))
+        fn = self._lib.tdda_matvec_c64 if precision == "complex64" else self._lib.tdda_matvec
+        _lib.check(fn(self._handle, _dp(xx.view(np.float64)), _dp(y.view(np.float64)), 1 if with_al else 0))
         return y
 
     def solve_batch_device(self, B_ptr, X_ptr, nrhs, x0_zero=True, max_iter=100000, tol=1e-8,

@@ -104,6 +104,7 @@ SIGNATURES = {
     "tdda_get_electric_field": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_int64]),
     "tdda_get_polarization": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_int64]),
     "tdda_matvec": (ctypes.c_int, [ctypes.c_void_p, _dp, _dp, ctypes.c_int]),
+    "tdda_matvec_c64": (ctypes.c_int, [ctypes.c_void_p, _dp, _dp, ctypes.c_int]),
     "tdda_solve_batch_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                                ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                                ctypes.c_void_p, ctypes.POINTER(SolveInfo)]),
