@@ -172,11 +172,19 @@ def peaks():
 
 
 def traffic_record():
-    path = os.path.join(ROOT, "profiles", "matvec_c64_traffic.json")
-    if os.path.exists(path):
-        with open(path) as f:
-            return json.load(f)
-    return None
+    """DRAM bytes per fused complex64 matvec from the committed ncu summary
+    (profiles/matvec_c64_traffic.txt: 'key: value' lines)."""
+    path = os.path.join(ROOT, "profiles", "matvec_c64_traffic.txt")
+    if not os.path.exists(path):
+        return None
+    rec = {}
+    with open(path) as f:
+        for line in f:
+            if line.startswith("#") or ":" not in line:
+                continue
+            k, v = line.split(":", 1)
+            rec[k.strip()] = float(v)
+    return rec
 
 
 def dist_setup():
@@ -447,7 +455,9 @@ def main():
                       "true_residual": [i["true_error"] for i in info_mixed]},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
-                         "traffic": (tr or {}).get("bytes_per_launch"),
+                         "traffic": (tr or {}).get("bytes_per_launch_cold"),
+                         "traffic_warm": (tr or {}).get("bytes_per_launch_warm"),
+                         "traffic_source": "profiles/matvec_c64_traffic.txt (ncu dram bytes, 3 passes, 1 RHS)",
                          "kernel": "fused complex64 matvec (3 passes), 1 RHS",
                          "algorithmic_bytes": b64, "ms": ms64, "pass_ms": pass64,
                          "c128": {"ms": ms128, "achieved": b128 / (ms128 * 1e-3) / 1e9, "pass_ms": pass128},

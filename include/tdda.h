@@ -156,6 +156,18 @@ tdda_status tdda_set_densities(tdda_model *m, const double *rho, int64_t n);
  * runs one adjoint solve, grad: double[N]. */
 tdda_status tdda_gradient_densities(tdda_model *m, int max_iter, double tol, double *grad, int64_t n,
                                     tdda_solve_info *info);
+/* Observation-patch objective (no reference counterpart; the nearest is
+ * ObjPointEDDAModel, src/ObjDDAModel.cpp:20-100, and the off-structure branch
+ * of DDAModel::solve_E, src/DDAModel.cpp:1154-1179): points xyz[3*nobs] in grid
+ * units, outside the dipoles.  E_obs = E_inc(r_o) - sum_j G(r_o - r_j) P_j with
+ * the model's damped periodic lattice sums; J = mean_o |E_obs|^2. */
+tdda_status tdda_set_observation_points(tdda_model *m, const int32_t *xyz, int64_t nobs);
+tdda_status tdda_observation_field(tdda_model *m, double *E, int64_t n);   /* complex[3*nobs] */
+tdda_status tdda_patch_objective(tdda_model *m, double *out);
+/* Exact adjoint gradient of the patch objective w.r.t. every dipole density
+ * (one adjoint solve with the same operator): grad double[N]. */
+tdda_status tdda_patch_gradient(tdda_model *m, int max_iter, double tol, double *grad, int64_t n,
+                                tdda_solve_info *info);
 /* Timing of the fused operator on the model's stream (CUDA events):
  * ms_matvec = mean time of one A.x (three kernels) for nrhs right-hand
  * sides, ms_pass[3] = mean time of each pass.  precision: 0 complex128,

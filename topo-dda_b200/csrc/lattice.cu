@@ -385,6 +385,83 @@ tdda_status build_tensor(const LatticeParams &P0, const double *si, const double
     return TDDA_OK;
 }
 
+// Lattice sums on an arbitrary box of integer offsets [lo, lo + n) (no
+// parity folding): out[((ix * ny) + iy) * nz + iz][6] for offset lo + (ix, iy, iz).
+// Used for fields at observation points outside the dipole box.
+__global__ void __launch_bounds__(LNT) k_lattice_box(LatticeParams P, int lox, int loy, int loz, int nbx, int nby,
+                                                     int nbz, double2 *__restrict__ out, int lanes) {
+    const long long gid = (long long)blockIdx.x * LNT + threadIdx.x;
+    const long long entry = gid / lanes;
+    const int lane = (int)(gid % lanes);
+    const long long nent = (long long)nbx * nby * nbz;
+    const bool valid = entry < nent;
+    int i = 0, j = 0, k = 0;
+    if (valid) {
+        i = (int)(entry / ((long long)nby * nbz));
+        int rem = (int)(entry - (long long)i * nby * nbz);
+        j = rem / nbz;
+        k = rem - j * nbz;
+    }
+    double acc[12];
+#pragma unroll
+    for (int l = 0; l < 12; ++l) acc[l] = 0.0;
+    if (valid) {
+        const double x0 = P.d * (lox + i), y0 = P.d * (loy + j), z = P.d * (loz + k);
+        const int nn = 2 * P.MAXn + 1;
+        const int nimg = (2 * P.MAXm + 1) * nn;
+        const double gk = P.gamma * P.K;
+        for (int q = lane; q < nimg; q += lanes) {
+            const int m = q / nn - P.MAXm;
+            const int n = q % nn - P.MAXn;
+            const double x = x0 + m * P.Lm, y = y0 + n * P.Ln;
+            const double r = sqrt(x * x + y * y + z * z);
+            if (r == 0.0) continue;
+            const double e = gk * r;
+            const double e2 = e * e, e4 = e2 * e2;
+            if (e4 > 746.0) continue;
+            const double damp = exp(-e4);
+            if (P.method == 0) fcd_term(x, y, z, r, damp, P, acc);
+            else ldr_term(x, y, z, r, damp, P, acc);
+        }
+    }
+    for (int off = lanes >> 1; off > 0; off >>= 1)
+#pragma unroll
+        for (int l = 0; l < 12; ++l) acc[l] += __shfl_down_sync(0xffffffffu, acc[l], off, lanes);
+    if (!valid || lane != 0) return;
+#pragma unroll
+    for (int l = 0; l < 6; ++l) out[(size_t)entry * 6 + l] = make_double2(acc[2 * l], acc[2 * l + 1]);
+}
+
+tdda_status build_offset_tensor(const LatticeParams &P0, const double *si, const double *ci, long ntab, int lox,
+                                int loy, int loz, int nbx, int nby, int nbz, double2 *out, cudaStream_t s) {
+    LatticeParams P = P0;
+    double2 *sc = nullptr;
+    std::vector<double2> h(ntab > 0 ? ntab : 1);
+    for (long q = 0; q < ntab; ++q) h[q] = make_double2(si[q], ci[q]);
+    if (cudaMalloc(&sc, sizeof(double2) * h.size()) != cudaSuccess) {
+        set_error("cannot upload the SiCi tables");
+        return TDDA_ERR_OOM;
+    }
+    cudaMemcpy(sc, h.data(), sizeof(double2) * h.size(), cudaMemcpyHostToDevice);
+    P.sc = sc;
+    P.ntab = ntab;
+    const long long nent = (long long)nbx * nby * nbz;
+    const long long nimg = (long long)(2 * P.MAXm + 1) * (2 * P.MAXn + 1);
+    int lanes = 1;
+    while (lanes < 32 && lanes < nimg) lanes <<= 1;
+    const long long threads = nent * lanes;
+    count_launches(1);
+    k_lattice_box<<<(unsigned)((threads + LNT - 1) / LNT), LNT, 0, s>>>(P, lox, loy, loz, nbx, nby, nbz, out, lanes);
+    cudaError_t err = cudaStreamSynchronize(s);
+    if (err == cudaSuccess) err = cudaGetLastError();
+    cudaFree(sc);
+    if (err != cudaSuccess) {
+        set_error(std::string("offset tensor: ") + cudaGetErrorString(err));
+        return TDDA_ERR_CUDA;
+    }
+    return TDDA_OK;
+}
+
 // Green tensor at arbitrary offsets (for tests of the lattice kernel against
 // the oracle's single-term evaluation): out[6] complex per offset.
 __global__ void k_green_points(LatticeParams P, const double *__restrict__ xyz, int npts, int m, int n,

@@ -29,4 +29,9 @@ tdda_status build_tensor(const LatticeParams &P, const double *si, const double 
                          double2 *ahat, float2 *ahat32, cudaStream_t s, double *lattice_ms,
                          double *fft_ms, double2 *a0);
 
+// Lattice sums (same periodic images and damping) for every integer offset
+// lo + (i, j, k), i < nbx, j < nby, k < nbz: out[((i*nby + j)*nbz + k)*6 + l].
+tdda_status build_offset_tensor(const LatticeParams &P, const double *si, const double *ci, long ntab, int lox,
+                                int loy, int loz, int nbx, int nby, int nbz, double2 *out, cudaStream_t s);
+
 }  // namespace tdda

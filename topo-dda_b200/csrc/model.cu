@@ -326,6 +326,114 @@ __global__ void k_grad_analytic(long long nbox, const double *__restrict__ rho, 
     }
 }
 
+// ---- observation patch -----------------------------------------------------
+// E_obs = E_inc(r_o) - sum_j G(r_o - r_j) P_j with G the same damped lattice
+// sum as the operator (offsets in grid units, tensor on the offset box).
+struct PatchGeo {
+    int nx, ny, nz;
+    int lox, loy, loz, bx, by, bz;
+};
+
+__device__ __forceinline__ const double2 *gobs_at(const double2 *G, const PatchGeo &pg, int dx, int dy, int dz) {
+    return G + ((size_t)((dx - pg.lox) * pg.by + (dy - pg.loy)) * pg.bz + (dz - pg.loz)) * 6;
+}
+
+// G (symmetric, components xx xy xz yy yz zz) times v, row c
+__device__ __forceinline__ double2 grow(const double2 *g, int c, double2 vx, double2 vy, double2 vz) {
+    const int i0 = c == 0 ? 0 : c == 1 ? 1 : 2;
+    const int i1 = c == 0 ? 1 : c == 1 ? 3 : 4;
+    const int i2 = c == 0 ? 2 : c == 1 ? 4 : 5;
+    double2 a = cmul_d(g[i0], vx), b = cmul_d(g[i1], vy), d = cmul_d(g[i2], vz);
+    return make_double2(a.x + b.x + d.x, a.y + b.y + d.y);
+}
+
+// one block per observation point; deterministic block reduction
+__global__ void k_patch_field(int nobs, const int *__restrict__ obs, PatchGeo pg, const unsigned char *__restrict__ mask,
+                              const double2 *__restrict__ P, long long nbox, const double2 *__restrict__ G,
+                              const double2 *__restrict__ Einc_obs, double2 *__restrict__ Eobs) {
+    const int o = blockIdx.x;
+    const int ox = obs[3 * o], oy = obs[3 * o + 1], oz = obs[3 * o + 2];
+    double2 acc[3] = {make_double2(0, 0), make_double2(0, 0), make_double2(0, 0)};
+    const int nyz = pg.ny * pg.nz;
+    for (long long cell = threadIdx.x; cell < nbox; cell += blockDim.x) {
+        if (mask != nullptr && mask[cell] == 0) continue;
+        const int x = (int)(cell / nyz), rem = (int)(cell - (long long)x * nyz);
+        const int y = rem / pg.nz, z = rem - y * pg.nz;
+        const double2 *g = gobs_at(G, pg, ox - x, oy - y, oz - z);
+        const double2 px = P[cell], py = P[nbox + cell], pz = P[2 * nbox + cell];
+        for (int c = 0; c < 3; ++c) {
+            double2 v = grow(g, c, px, py, pz);
+            acc[c].x += v.x;
+            acc[c].y += v.y;
+        }
+    }
+    __shared__ double2 red[3][32];
+    for (int c = 0; c < 3; ++c)
+        for (int off = 16; off > 0; off >>= 1) {
+            acc[c].x += __shfl_xor_sync(0xffffffffu, acc[c].x, off);
+            acc[c].y += __shfl_xor_sync(0xffffffffu, acc[c].y, off);
+        }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if (lane == 0)
+        for (int c = 0; c < 3; ++c) red[c][wid] = acc[c];
+    __syncthreads();
+    if (wid == 0) {
+        for (int c = 0; c < 3; ++c) {
+            double2 v = lane < nw ? red[c][lane] : make_double2(0, 0);
+            for (int off = 16; off > 0; off >>= 1) {
+                v.x += __shfl_xor_sync(0xffffffffu, v.x, off);
+                v.y += __shfl_xor_sync(0xffffffffu, v.y, off);
+            }
+            if (lane == 0) {
+                const double2 e = Einc_obs[3 * o + c];
+                Eobs[3 * o + c] = make_double2(e.x - v.x, e.y - v.y);
+            }
+        }
+    }
+}
+
+// adjoint right-hand side of J = (1/nobs) sum_o |E_o|^2:
+// dJ/dx - i dJ/dy at dipole j = -(2/nobs) sum_o G(r_o - r_j) conj(E_o)
+__global__ void k_patch_adjoint_rhs(int nobs, const int *__restrict__ obs, PatchGeo pg,
+                                    const unsigned char *__restrict__ mask, long long nbox,
+                                    const double2 *__restrict__ G, const double2 *__restrict__ Eobs,
+                                    double2 *__restrict__ rhs) {
+    const int nyz = pg.ny * pg.nz;
+    const double w = -2.0 / nobs;
+    for (long long cell = (long long)blockIdx.x * blockDim.x + threadIdx.x; cell < nbox;
+         cell += (long long)gridDim.x * blockDim.x) {
+        double2 acc[3] = {make_double2(0, 0), make_double2(0, 0), make_double2(0, 0)};
+        if (mask == nullptr || mask[cell] != 0) {
+            const int x = (int)(cell / nyz), rem = (int)(cell - (long long)x * nyz);
+            const int y = rem / pg.nz, z = rem - y * pg.nz;
+            for (int o = 0; o < nobs; ++o) {
+                const double2 *g = gobs_at(G, pg, obs[3 * o] - x, obs[3 * o + 1] - y, obs[3 * o + 2] - z);
+                const double2 ex = conj(Eobs[3 * o]), ey = conj(Eobs[3 * o + 1]), ez = conj(Eobs[3 * o + 2]);
+                for (int c = 0; c < 3; ++c) {
+                    double2 v = grow(g, c, ex, ey, ez);
+                    acc[c].x += v.x;
+                    acc[c].y += v.y;
+                }
+            }
+        }
+        for (int c = 0; c < 3; ++c) rhs[(size_t)c * nbox + cell] = make_double2(w * acc[c].x, w * acc[c].y);
+    }
+}
+
+// gradient of an objective without explicit density dependence:
+// dJ/drho_j = -Re(sum_c lambda_jc al'_j P_jc)
+__global__ void k_grad_implicit(long long nbox, const unsigned char *__restrict__ mask, const double2 *__restrict__ P,
+                                const double2 *__restrict__ diel, const double2 *__restrict__ lam, AlphaParams A,
+                                double *__restrict__ grad) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nbox; i += (long long)gridDim.x * blockDim.x) {
+        if (mask != nullptr && mask[i] == 0) { grad[i] = 0.0; continue; }
+        const double2 da = dal_drho(diel[i], A);
+        double s = 0.0;
+        for (int c = 0; c < 3; ++c) s += cmul_d(lam[(size_t)c * nbox + i], cmul_d(da, P[(size_t)c * nbox + i])).x;
+        grad[i] = -s;
+    }
+}
+
 static unsigned grid_for(long long n, int bs = 256, unsigned cap = 148 * 16) {
     long long g = (n + bs - 1) / bs;
     if (g < 1) g = 1;
@@ -397,6 +505,16 @@ struct tdda_model {
     float2 *sc32 = nullptr, *alS32 = nullptr;
     SolverState *st_res = nullptr, *st_res_host = nullptr;
     double *d_part = nullptr, *h_part = nullptr;
+    // lattice inputs kept for later tensors (observation patches)
+    LatticeParams lat{};
+    std::vector<double> si_h, ci_h;
+    // observation patch: E_obs = E_inc(r_obs) - sum_j G(r_obs - r_j) P_j
+    int nobs = 0;
+    int *d_obs = nullptr;        // 3 ints per observation point (grid units)
+    double2 *Gobs = nullptr;     // lattice sums on the offset box [bx][by][bz][6]
+    int obs_lo[3]{}, obs_n[3]{};
+    double2 *Einc_obs = nullptr; // [nobs][3]
+    double2 *Eobs = nullptr;     // [nobs][3]
     // stats
     double lattice_ms = 0, fft_ms = 0;
     long long device_bytes = 0;
@@ -406,8 +524,9 @@ struct tdda_model {
         op32.release();
         kv.release();
         kv32.release();
-        void *bufs[] = {d_cell, d_mask, d_rho, al,    diel,  al32, Einc, P,    Eres,  ext,   bufB, bufX,  Rm,
-                        R32,    D32,    st_res, d_part, R64, D64,  sc64, alS64, sc32, alS32};
+        void *bufs[] = {d_cell, d_mask, d_rho,  al,  diel, al32,  Einc, P,     Eres,  ext,   bufB,     bufX,
+                        Rm,     R32,    D32,    st_res, d_part, R64, D64,  sc64, alS64, sc32, alS32, d_obs,
+                        Gobs,   Einc_obs, Eobs};
         for (void *b : bufs) cudaFree(b);
         cudaFreeHost(st_res_host);
         cudaFreeHost(h_part);
@@ -880,6 +999,9 @@ tdda_status tdda_model_create(const tdda_params *p, const int32_t *geometry, con
     long nt = (si && ci) ? (long)ntab : 2;
     double2 a0[6];
     TRY(build_tensor(L, tsi, tci, nt, m->op.ahat, ahat32, m->stream, &m->lattice_ms, &m->fft_ms, a0));
+    m->lat = L;
+    m->si_h.assign(tsi, tsi + nt);
+    m->ci_h.assign(tci, tci + nt);
     m->a0 = make_double2((a0[0].x + a0[3].x + a0[5].x) / 3.0, (a0[0].y + a0[3].y + a0[5].y) / 3.0);
 
     // incident field (src/DDAModel.cpp:312-316), internal layout
@@ -1251,6 +1373,120 @@ tdda_status tdda_set_preconditioner(tdda_model *m, int kind) {
     if (!m) return bad("null model");
     if (kind != 0 && kind != 1) return bad("preconditioner must be 0 (none) or 1 (Jacobi)");
     m->precond = kind;
+    return TDDA_OK;
+}
+
+tdda_status tdda_set_observation_points(tdda_model *m, const int32_t *xyz, int64_t nobs) {
+    if (!m || !xyz || nobs < 1) return bad("bad argument");
+    if (nobs > 1 << 20) return bad("too many observation points");
+    int lo[3], hi[3];
+    const int nb[3] = {m->Nx, m->Ny, m->Nz};
+    for (int a = 0; a < 3; ++a) {
+        lo[a] = INT32_MAX;
+        hi[a] = INT32_MIN;
+    }
+    std::vector<double2> einc(3 * (size_t)nobs);
+    for (int64_t o = 0; o < nobs; ++o) {
+        bool inside = true;
+        for (int a = 0; a < 3; ++a) {
+            lo[a] = std::min(lo[a], xyz[3 * o + a] - (nb[a] - 1));
+            hi[a] = std::max(hi[a], (int)xyz[3 * o + a]);
+            inside &= (xyz[3 * o + a] >= 0 && xyz[3 * o + a] < nb[a]);
+        }
+        if (inside) {
+            long long cell = ((long long)xyz[3 * o] * m->Ny + xyz[3 * o + 1]) * m->Nz + xyz[3 * o + 2];
+            if (m->d_mask == nullptr || m->N == m->nbox) return bad("observation point on a dipole");
+            (void)cell;
+        }
+        // incident plane wave at the point (src/DDAModel.cpp:312-316 for a grid position)
+        const double ph = m->K * m->d * (m->nK[0] * xyz[3 * o] + m->nK[1] * xyz[3 * o + 1] + m->nK[2] * xyz[3 * o + 2]);
+        for (int c = 0; c < 3; ++c)
+            einc[3 * o + c] = make_double2(m->E0 * m->nE0[c] * std::cos(ph), m->E0 * m->nE0[c] * std::sin(ph));
+    }
+    int n[3];
+    long long total = 1;
+    for (int a = 0; a < 3; ++a) {
+        n[a] = hi[a] - lo[a] + 1;
+        total *= n[a];
+    }
+    if (total > (1LL << 27)) return bad("observation points span too large an offset box");
+    cudaFree(m->d_obs); cudaFree(m->Gobs); cudaFree(m->Einc_obs); cudaFree(m->Eobs);
+    m->d_obs = nullptr; m->Gobs = m->Einc_obs = m->Eobs = nullptr; m->nobs = 0;
+    TDDA_CUDA_TRY(cudaMalloc(&m->d_obs, sizeof(int) * 3 * nobs));
+    TDDA_CUDA_TRY(cudaMemcpy(m->d_obs, xyz, sizeof(int) * 3 * nobs, cudaMemcpyHostToDevice));
+    TDDA_CUDA_TRY(cudaMalloc(&m->Gobs, sizeof(double2) * 6 * total));
+    TDDA_CUDA_TRY(cudaMalloc(&m->Einc_obs, sizeof(double2) * 3 * nobs));
+    TDDA_CUDA_TRY(cudaMalloc(&m->Eobs, sizeof(double2) * 3 * nobs));
+    TDDA_CUDA_TRY(cudaMemcpy(m->Einc_obs, einc.data(), sizeof(double2) * 3 * nobs, cudaMemcpyHostToDevice));
+    TRY(build_offset_tensor(m->lat, m->si_h.data(), m->ci_h.data(), (long)m->si_h.size(), lo[0], lo[1], lo[2], n[0],
+                            n[1], n[2], m->Gobs, m->stream));
+    for (int a = 0; a < 3; ++a) {
+        m->obs_lo[a] = lo[a];
+        m->obs_n[a] = n[a];
+    }
+    m->nobs = (int)nobs;
+    return TDDA_OK;
+}
+
+static PatchGeo patch_geo(const tdda_model *m) {
+    return {m->Nx, m->Ny, m->Nz, m->obs_lo[0], m->obs_lo[1], m->obs_lo[2], m->obs_n[0], m->obs_n[1], m->obs_n[2]};
+}
+
+static tdda_status patch_field(tdda_model *m) {
+    if (m->nobs == 0) {
+        set_error("no observation points: call tdda_set_observation_points first");
+        return TDDA_ERR_STATE;
+    }
+    count_launches(1);
+    k_patch_field<<<m->nobs, 256, 0, m->stream>>>(m->nobs, m->d_obs, patch_geo(m), m->d_mask, m->P, m->nbox,
+                                                  m->Gobs, m->Einc_obs, m->Eobs);
+    TDDA_CUDA_TRY(cudaGetLastError());
+    return TDDA_OK;
+}
+
+tdda_status tdda_observation_field(tdda_model *m, double *E, int64_t n) {
+    if (!m || !E) return bad("null argument");
+    if (n != 3LL * m->nobs) return bad("buffer must hold 3 complex values per observation point");
+    TRY(patch_field(m));
+    TDDA_CUDA_TRY(cudaMemcpyAsync(E, m->Eobs, sizeof(double2) * 3 * m->nobs, cudaMemcpyDeviceToHost, m->stream));
+    TDDA_CUDA_TRY(cudaStreamSynchronize(m->stream));
+    return TDDA_OK;
+}
+
+tdda_status tdda_patch_objective(tdda_model *m, double *out) {
+    if (!m || !out) return bad("null argument");
+    std::vector<double2> e(3 * (size_t)m->nobs);
+    TRY(tdda_observation_field(m, reinterpret_cast<double *>(e.data()), 3LL * m->nobs));
+    double s = 0.0;
+    for (const double2 &v : e) s += v.x * v.x + v.y * v.y;
+    *out = s / m->nobs;
+    return TDDA_OK;
+}
+
+tdda_status tdda_patch_gradient(tdda_model *m, int max_iter, double tol, double *grad, int64_t n,
+                                tdda_solve_info *info) {
+    if (!m || !grad) return bad("null argument");
+    if (n != m->N) return bad("gradient buffer must hold N values");
+    TRY(patch_field(m));
+    TRY(ensure_batch(m, 1));
+    const long long nbox = m->nbox;
+    count_launches(1);
+    k_patch_adjoint_rhs<<<grid_for(nbox), 256, 0, m->stream>>>(m->nobs, m->d_obs, patch_geo(m), m->d_mask, nbox,
+                                                                m->Gobs, m->Eobs, m->bufB);
+    TDDA_CUDA_TRY(cudaGetLastError());
+    tdda_solve_info inf{};
+    TRY(solve_internal(m, m->bufB, m->bufX, 1, true, max_iter, tol, &inf));
+    double *g = nullptr;
+    TDDA_CUDA_TRY(cudaMalloc(&g, sizeof(double) * nbox));
+    std::unique_ptr<void, void (*)(void *)> gg(g, [](void *p) { cudaFree(p); });
+    count_launches(1);
+    k_grad_implicit<<<grid_for(nbox), 256, 0, m->stream>>>(nbox, m->d_mask, m->P, m->diel, m->bufX, m->ap, g);
+    TDDA_CUDA_TRY(cudaGetLastError());
+    std::vector<double> h(nbox);
+    TDDA_CUDA_TRY(cudaMemcpyAsync(h.data(), g, sizeof(double) * nbox, cudaMemcpyDeviceToHost, m->stream));
+    TDDA_CUDA_TRY(cudaStreamSynchronize(m->stream));
+    for (int i = 0; i < m->N; ++i) grad[i] = h[m->cell_of[i]];
+    if (info) *info = inf;
     return TDDA_OK;
 }
 

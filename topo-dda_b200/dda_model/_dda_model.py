@@ -197,6 +197,33 @@ class DDAModel:
         self.last_adjoint = info.as_dict()
         return g
 
+    def setObservationPoints(self, xyz):
+        """Observation points (grid units, shape [nobs, 3]) for the patch objective."""
+        a = np.ascontiguousarray(np.asarray(xyz).reshape(-1, 3).astype(np.int32))
+        _lib.check(self._lib.tdda_set_observation_points(self._handle, a.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                                                          a.shape[0]))
+        self.nobs = a.shape[0]
+
+    def observationField(self):
+        e = np.zeros(3 * self.nobs, dtype=np.complex128)
+        _lib.check(self._lib.tdda_observation_field(self._handle, _dp(e.view(np.float64)), e.size))
+        return e
+
+    def patchObjective(self):
+        """mean over observation points of |E|^2 (uses the last solve)."""
+        out = ctypes.c_double()
+        _lib.check(self._lib.tdda_patch_objective(self._handle, ctypes.byref(out)))
+        return out.value
+
+    def patchGradient(self, max_iter=100000, tol=1e-10):
+        """Exact adjoint gradient of patchObjective w.r.t. every dipole density."""
+        g = np.zeros(self.N)
+        info = _lib.SolveInfo()
+        _lib.check(self._lib.tdda_patch_gradient(self._handle, int(max_iter), float(tol), _dp(g), g.size,
+                                                 ctypes.byref(info)))
+        self.last_adjoint = info.as_dict()
+        return g
+
     def profile_matvec(self, precision="complex128", nrhs=1, iters=20):
         """Device time of one operator application (ms) and of each of its 3 passes."""
         tot = ctypes.c_double()

@@ -118,6 +118,11 @@ SIGNATURES = {
     "tdda_kernel_launches": (ctypes.c_longlong, []),
     "tdda_set_precision": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "tdda_set_preconditioner": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "tdda_set_observation_points": (ctypes.c_int, [ctypes.c_void_p, _ip, ctypes.c_int64]),
+    "tdda_observation_field": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_int64]),
+    "tdda_patch_objective": (ctypes.c_int, [ctypes.c_void_p, _dp]),
+    "tdda_patch_gradient": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, _dp, ctypes.c_int64,
+                                           ctypes.POINTER(SolveInfo)]),
     "tdda_matvec_device_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                                   ctypes.c_int, ctypes.c_void_p]),
 }
