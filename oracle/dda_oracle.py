@@ -77,6 +77,10 @@ def _load_lib():
         lib.oracle_get_ci.argtypes = [dp, ctypes.c_long, ctypes.c_double, ctypes.c_double]
         lib.oracle_get_ci.restype = ctypes.c_double
         lib.oracle_guard_hits.restype = ctypes.c_long
+        lib.oracle_lattice_points.argtypes = [
+            ctypes.c_int, ctypes.c_long, dp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+            ctypes.c_double, ctypes.c_double, dp, dp, ctypes.c_long, ctypes.c_double, dp,
+        ]
         _lib = lib
     return _lib
 
@@ -499,6 +503,79 @@ class OracleModel:
         mult = np.zeros(self.NFpara, dtype=np.complex128)
         np.add.at(mult, self.geometryPara, prod)
         return devx - mult.real
+
+    # --- observation patch (extension objective; no reference counterpart) ------
+    def observation_matrix(self, obs):
+        """Gobs[3 nobs, 3N]: the damped periodic lattice sum G(r_o - r_j) between
+        every observation grid point r_o and every dipole r_j (component blocks
+        xx,xy,xz / yx,yy,yz / zx,zy,zz)."""
+        lib = _load_lib()
+        g = self.geometry.reshape(-1, 3)
+        obs = np.asarray(obs).reshape(-1, 3)
+        comp = [[0, 1, 2], [1, 3, 4], [2, 4, 5]]
+        G = np.zeros((3 * len(obs), 3 * self.N), dtype=np.complex128)
+        for k, o in enumerate(obs):
+            off = np.ascontiguousarray(((o[None, :] - g) * self.d).astype(np.float64))
+            out = np.zeros(12 * len(g))
+            lib.oracle_lattice_points({"FCD": 0, "LDR": 1}[self.method], len(g), _dptr(off), self.MAXm,
+                                      self.MAXn, self.Lm, self.Ln, self.K, self.d, _dptr(self.si),
+                                      _dptr(self.ci), len(self.si), self.delta, _dptr(out))
+            T = out.view(np.complex128).reshape(-1, 6)
+            for a in range(3):
+                for b in range(3):
+                    G[3 * k + a, b::3] = T[:, comp[a][b]]
+        return G
+
+    def observation_field(self, obs):
+        """E_obs = E_inc(r_o) - sum_j G(r_o - r_j) P_j at grid points obs[nobs, 3]."""
+        obs = np.asarray(obs).reshape(-1, 3)
+        ph = self.K * self.d * (obs.astype(np.float64) @ self.n_K)
+        Einc = self.E0 * self.n_E0[None, :] * np.exp(1j * ph)[:, None]
+        return Einc - (self.observation_matrix(obs) @ self.P).reshape(-1, 3)
+
+    def patch_objective(self, obs):
+        E = self.observation_field(obs)
+        return float(np.sum(np.abs(E) ** 2) / len(E))
+
+    # --- per-dipole densities (extension of setParameters) ----------------------
+    def set_densities(self, rho):
+        """Free per-dipole densities (no symmetry map): rho[N] -> diel, 1/alpha."""
+        rho = np.asarray(rho, dtype=np.float64)
+        if rho.shape != (self.N,):
+            raise RuntimeError("densities must have num_total entries")
+        self.dielectric_old = np.repeat(rho, 3)
+        self.diel = interp_material(self.dielectric_old, self.material)
+        self.al = 1.0 / get_alpha(self.lam, self.K, self.d, self.diel, self.n_E0, self.n_K)
+
+    def density_gradient(self, kind="integrated", obs=None):
+        """Exact dJ/drho_j by a dense direct forward and adjoint solve (small N).
+
+        (A + diag al) P = E with a complex-symmetric matrix, so for
+        J(P, al): dJ/drho_j = Re(sum_c [dJ/dal_jc - lambda_jc P_jc] dal_j/drho_j)
+        with (A + diag al) lambda = v, v = dJ/dP (holomorphic part)."""
+        M = self.dense_operator()
+        P = np.linalg.solve(M, self.E)
+        self.P = P
+        if kind == "integrated":
+            q = self.powNum
+            z = self.al * P
+            S = float(np.sum(np.abs(z) ** q))
+            w = q * np.abs(z) ** (q - 2) * np.conj(z)  # d|z|^q = Re(w dz)
+            v = w * self.al / S
+            explicit = w * P / S
+        elif kind == "patch":
+            G = self.observation_matrix(obs)
+            nobs = G.shape[0] // 3
+            ph = self.K * self.d * (np.asarray(obs).reshape(-1, 3).astype(np.float64) @ self.n_K)
+            Einc = (self.E0 * self.n_E0[None, :] * np.exp(1j * ph)[:, None]).ravel()
+            E = Einc - G @ P
+            v = -(2.0 / nobs) * (G.T @ np.conj(E))
+            explicit = np.zeros(3 * self.N, dtype=np.complex128)
+        else:
+            raise ValueError(kind)
+        lam = np.linalg.solve(M, v)  # M^T = M
+        per = (explicit - lam * P).reshape(-1, 3).sum(axis=1)
+        return (per * self.dal_drho()).real
 
     # --- analytic derivative (used to check the analytic adjoint) ---------------
     def dal_drho(self):

@@ -294,3 +294,16 @@ int oracle_lattice(int Nx, int Ny, int Nz, double d, double K, double Lm, double
 double oracle_get_si(const double *si, long n, double delta, double x) { return sici_lookup(si, n, delta, x); }
 double oracle_get_ci(const double *ci, long n, double delta, double x) { return sici_lookup(ci, n, delta, x); }
 long oracle_guard_hits(void) { return oracle_sici_guard_hits; }
+
+/* Lattice sums (same images and damping as the tensor entries) at arbitrary
+ * offsets xyz[3*npts] (lengths): out[12*npts], components xx,xy,xz,yy,yz,zz.
+ * Used for fields at observation points outside the dipole grid. */
+int oracle_lattice_points(int method, long npts, const double *xyz, int MAXm, int MAXn, double Lm, double Ln,
+                          double K, double d, const double *si, const double *ci, long ntab, double delta,
+                          double *out)
+{
+    for (long p = 0; p < npts; p++)
+        entry_sum(method, xyz[3 * p], xyz[3 * p + 1], xyz[3 * p + 2], MAXm, MAXn, Lm, Ln, K, d, si, ci, ntab,
+                  delta, out + 12 * p);
+    return 0;
+}

@@ -106,3 +106,31 @@ def test_reference_gradient_close_to_analytic_adjoint(sici):
             m.solveElectricField(np.zeros(3 * m.N, complex), 1000, 1e-13)
             vals.append(m.calculateObjective())
         assert (vals[0] - vals[1]) / (2 * h) == pytest.approx(exact[k], rel=1e-5)
+
+
+@pytest.mark.parametrize("kind", ["integrated", "patch"])
+def test_density_gradient_matches_central_differences(sici, kind):
+    """The oracle's dense exact-adjoint density gradient (the checker of the
+    CUDA adjoint) against central differences of the directly solved objective."""
+    from oracle.dda_oracle import OracleModel
+
+    m = OracleModel(**model_args(4, 4, 2, sici, MAXm=1, MAXn=1, seed=11))
+    obs = np.array([[x, y, 4] for x in (1, 2) for y in (1, 3)])
+    rho = np.random.default_rng(12).uniform(0.1, 0.9, m.N)
+
+    def J(r):
+        m.set_densities(r)
+        m.P = np.linalg.solve(m.dense_operator(), m.E)
+        if kind == "integrated":
+            return m.calculateObjective()
+        return m.patch_objective(obs)
+
+    m.set_densities(rho)
+    g = m.density_gradient(kind, obs)
+    assert g.shape == (m.N,)
+    h = 1e-6
+    for j in (0, 5, m.N - 1):
+        e = np.zeros(m.N)
+        e[j] = h
+        fd = (J(rho + e) - J(rho - e)) / (2 * h)
+        assert abs(fd - g[j]) <= 1e-6 * np.abs(g).max()

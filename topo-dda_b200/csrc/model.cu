@@ -1386,6 +1386,7 @@ tdda_status tdda_set_observation_points(tdda_model *m, const int32_t *xyz, int64
         hi[a] = INT32_MIN;
     }
     std::vector<double2> einc(3 * (size_t)nobs);
+    std::vector<char> occupied;  // built on the first point inside the box
     for (int64_t o = 0; o < nobs; ++o) {
         bool inside = true;
         for (int a = 0; a < 3; ++a) {
@@ -1394,9 +1395,12 @@ tdda_status tdda_set_observation_points(tdda_model *m, const int32_t *xyz, int64
             inside &= (xyz[3 * o + a] >= 0 && xyz[3 * o + a] < nb[a]);
         }
         if (inside) {
-            long long cell = ((long long)xyz[3 * o] * m->Ny + xyz[3 * o + 1]) * m->Nz + xyz[3 * o + 2];
-            if (m->d_mask == nullptr || m->N == m->nbox) return bad("observation point on a dipole");
-            (void)cell;
+            if (occupied.empty()) {
+                occupied.assign(m->nbox, 0);
+                for (long long c : m->cell_of) occupied[c] = 1;
+            }
+            const long long cell = ((long long)xyz[3 * o] * m->Ny + xyz[3 * o + 1]) * m->Nz + xyz[3 * o + 2];
+            if (occupied[cell]) return bad("observation point on a dipole");
         }
         // incident plane wave at the point (src/DDAModel.cpp:312-316 for a grid position)
         const double ph = m->K * m->d * (m->nK[0] * xyz[3 * o] + m->nK[1] * xyz[3 * o + 1] + m->nK[2] * xyz[3 * o + 2]);

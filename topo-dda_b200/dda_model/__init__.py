@@ -9,8 +9,9 @@ from __future__ import annotations
 import numpy as np
 
 from ._dda_model import DDAModel
+from ._lib import TddaError
 
-__all__ = ["DDAModel", "DDAModelWrapper", "_generate_geometry", "sici_tables"]
+__all__ = ["DDAModel", "DDAModelWrapper", "TddaError", "_generate_geometry", "sici_tables"]
 
 
 def _generate_geometry(num_x: int, num_y: int, num_z: int) -> np.ndarray:

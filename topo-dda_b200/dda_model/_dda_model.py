@@ -111,11 +111,14 @@ class DDAModel:
 
     # --- the reference's seven methods -----------------------------------------
     def solveElectricField(self, originPolarization, BGS_MAX_ITER, BGS_MAX_ERROR):
-        """src/DDAModel.cpp:874-885."""
-        p0 = _c128(originPolarization, 3 * self.N, "originPolarization")
+        """src/DDAModel.cpp:874-885 (originPolarization=None: zero initial guess)."""
+        if originPolarization is None:
+            ptr = None
+        else:
+            p0 = _c128(originPolarization, 3 * self.N, "originPolarization")
+            ptr = _dp(p0.view(np.float64))
         info = _lib.SolveInfo()
-        _lib.check(self._lib.tdda_solve_electric_field(self._handle, _dp(p0.view(np.float64)),
-                                                       int(BGS_MAX_ITER), float(BGS_MAX_ERROR),
+        _lib.check(self._lib.tdda_solve_electric_field(self._handle, ptr, int(BGS_MAX_ITER), float(BGS_MAX_ERROR),
                                                        ctypes.byref(info)))
         self.last_solve = info.as_dict()
         return None
