@@ -202,6 +202,89 @@ tdda_status tdda_set_preconditioner(tdda_model *m, int kind);
 tdda_status tdda_matvec_device_noalloc(tdda_model *m, const void *x_dev, void *y_dev, int with_al,
                                        void *stream);
 
+/* ---------------------------------------------------------------------------
+ * Serving engine (no counterpart in the reference: its path solves one
+ * structure at a time in one process).  A server owns one GPU and runs a
+ * request loop with continuous batching:
+ *   - requests are queued at submit and admitted when a worker slot is free and
+ *     their device memory fits hbm_budget_bytes (interaction tensors +
+ *     per-worker solve workspaces);
+ *   - the FFT'd interaction tensor of each (grid, d, lambda, nback, period,
+ *     method) stays resident and is reused by later requests with the same key;
+ *     idle tensors are evicted least-recently-used when the budget is short;
+ *   - queued requests with the same key are merged with the admitted one into
+ *     one multi-right-hand-side solve (each polarisation is a right-hand side
+ *     with its own polarisability), up to max_rhs right-hand sides;
+ *   - each worker drives its batches on its own CUDA stream, so batches of
+ *     different workers overlap on the device; BiCGSTAB iterations are replayed
+ *     from CUDA graphs when use_graphs is set.
+ * Structures are full boxes num_x*num_y*num_z with per-dipole densities.
+ * ------------------------------------------------------------------------- */
+#define TDDA_SERVER_MAX_POL 4
+
+typedef struct tdda_server tdda_server;
+
+typedef struct {
+    int64_t hbm_budget_bytes; /* admission budget for tensors + workspaces */
+    int32_t workers;          /* concurrent batches (host thread + CUDA stream each), 1..64 */
+    int32_t max_rhs;          /* right-hand sides merged into one batched solve, 1..16 */
+    int32_t use_graphs;       /* replay BiCGSTAB iterations from CUDA graphs */
+    int32_t graph_steps;      /* iterations per graph (default 4 when 0) */
+} tdda_server_config;
+
+typedef struct {
+    int32_t num_x, num_y, num_z;  /* box; dipole i = x + num_x*(y + num_y*z) */
+    double d, lam, nback, E0;
+    double material[4];           /* background, structure: (re, im) each */
+    int32_t MAXm, MAXn;           /* periodic images |m| <= MAXm, |n| <= MAXn */
+    double Lm, Ln;                /* periods in units of d */
+    int32_t method;               /* 0 FCD, 1 LDR (polarisability: LDR for both) */
+    double n_K[3];                /* propagation direction of the plane wave */
+    int32_t npol;                 /* polarisations = right-hand sides, 1..TDDA_SERVER_MAX_POL */
+    double n_E0[TDDA_SERVER_MAX_POL][3];
+    const double *rho;            /* num_x*num_y*num_z densities in [0, 1] (copied at submit) */
+    int32_t precision;            /* TDDA_PREC_MIXED or TDDA_PREC_C128 (Jacobi-refined) */
+    double tol;                   /* true relative residual per right-hand side */
+    int32_t max_iter;
+    double *P_out;                /* npol*3N complex, dipole order, or NULL; valid until wait returns */
+    double *E_out;                /* npol*3N complex E_int = al P / ((2+eps)/3), or NULL */
+} tdda_request;
+
+typedef struct {
+    int32_t status;               /* tdda_status of the request */
+    tdda_solve_info info[TDDA_SERVER_MAX_POL];
+    int32_t batch_rhs;            /* right-hand sides of the batch it ran in */
+    int32_t batch_requests;       /* requests of that batch */
+    int32_t cache_hit;            /* its tensor was resident */
+    int32_t worker;
+    double queue_ms;              /* submit -> admitted */
+    double build_ms;              /* tensor build (0 on a hit) */
+    double solve_ms;              /* batch solve incl. setup and result copies */
+    double total_ms;              /* submit -> result ready */
+} tdda_request_result;
+
+typedef struct {
+    int64_t submitted, completed, failed;
+    int64_t cache_hits, cache_misses, evictions;
+    int64_t batches, merged_requests;   /* requests that joined another's batch */
+    int64_t bytes_in_use, peak_bytes, cached_tensors;
+    int32_t max_concurrent;             /* most batches in flight at once */
+    int32_t admission_waits;            /* times the queue head waited for memory */
+} tdda_server_stats;
+
+/* si, ci: the SiCi tables of tdda_model_create (shared by every FCD request). */
+tdda_status tdda_server_create(const tdda_server_config *cfg, const double *si, const double *ci, int64_t ntab,
+                               tdda_server **out);
+/* Queues a request; returns at once with its ticket.  Requests that can never
+ * fit the budget fail at submit with TDDA_ERR_OOM. */
+tdda_status tdda_server_submit(tdda_server *s, const tdda_request *req, int64_t *ticket);
+/* Waits up to timeout_s (< 0: forever) for a ticket; TDDA_ERR_TIMEOUT if not
+ * ready.  A ticket can be waited for once. */
+tdda_status tdda_server_wait(tdda_server *s, int64_t ticket, double timeout_s, tdda_request_result *result);
+tdda_status tdda_server_get_stats(tdda_server *s, tdda_server_stats *stats);
+/* Finishes queued work, then frees every device buffer. */
+void tdda_server_destroy(tdda_server *s);
+
 #ifdef __cplusplus
 }
 #endif

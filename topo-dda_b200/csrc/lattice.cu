@@ -277,56 +277,90 @@ static int pick_tile(int L, int want) {
     return t;
 }
 
-tdda_status build_tensor(const LatticeParams &P0, const double *si, const double *ci, long ntab,
-                         double2 *ahat, float2 *ahat32, cudaStream_t s, double *lattice_ms,
-                         double *fft_ms, double2 *a0) {
-    LatticeParams P = P0;
-    const size_t Lxyz = (size_t)P.Lx * P.Ly * P.Lz;
-    double2 *G = nullptr, *sc = nullptr, *tw = nullptr;
-    cudaEvent_t e0, e1, e2;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
-    cudaEventCreate(&e2);
-    auto cleanup = [&]() {
-        cudaFree(G);
-        cudaFree(sc);
-        cudaFree(tw);
-        cudaEventDestroy(e0);
-        cudaEventDestroy(e1);
-        cudaEventDestroy(e2);
-    };
-    {
-        std::vector<double2> h(ntab > 0 ? ntab : 1);
-        for (long q = 0; q < ntab; ++q) h[q] = make_double2(si[q], ci[q]);
-        if (cudaMalloc(&sc, sizeof(double2) * h.size()) != cudaSuccess ||
-            cudaMemcpy(sc, h.data(), sizeof(double2) * h.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
-            cleanup();
-            set_error("cannot upload the SiCi tables");
-            return TDDA_ERR_OOM;
-        }
-    }
-    P.sc = sc;
-    P.ntab = ntab;
-    if (cudaMalloc(&G, sizeof(double2) * 6 * Lxyz) != cudaSuccess) {
-        cleanup();
-        set_error("cannot allocate the padded tensor grid");
+static int lmax_of(int Lx, int Ly, int Lz) {
+    auto g = [](int a, int b) { while (b) { int t = a % b; a = b; b = t; } return a; };
+    int L = Lx;
+    L = L / g(L, Ly) * Ly;
+    L = L / g(L, Lz) * Lz;
+    return L;
+}
+
+tdda_status TensorScratch::init_tables(const double *si, const double *ci, long n) {
+    std::vector<double2> h(n > 0 ? n : 1, make_double2(0.0, 0.0));
+    for (long q = 0; q < n; ++q) h[q] = make_double2(si[q], ci[q]);
+    if (cudaMalloc(&sc, sizeof(double2) * h.size()) != cudaSuccess ||
+        cudaMemcpy(sc, h.data(), sizeof(double2) * h.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+        set_error("cannot upload the SiCi tables");
         return TDDA_ERR_OOM;
     }
-    int Lmax = P.Lx;
-    {
-        auto g = [](int a, int b) { while (b) { int t = a % b; a = b; b = t; } return a; };
-        Lmax = Lmax / g(Lmax, P.Ly) * P.Ly;
-        Lmax = Lmax / g(Lmax, P.Lz) * P.Lz;
-        std::vector<double2> h(Lmax);
-        for (int j = 0; j < Lmax; ++j) {
-            long double ang = -2.0L * 3.141592653589793238462643383279502884L * (long double)j / Lmax;
-            h[j] = make_double2((double)cosl(ang), (double)sinl(ang));
+    ntab = n;
+    owns_tables = true;
+    return TDDA_OK;
+}
+
+tdda_status TensorScratch::reserve(size_t Lxyz, int Lmax) {
+    if (G_elems < 6 * Lxyz) {
+        cudaFree(G);
+        G = nullptr;
+        G_elems = 0;
+        if (cudaMalloc(&G, sizeof(double2) * 6 * Lxyz) != cudaSuccess) {
+            set_error("cannot allocate the padded tensor grid");
+            return TDDA_ERR_OOM;
         }
-        cudaMalloc(&tw, sizeof(double2) * Lmax);
-        cudaMemcpy(tw, h.data(), sizeof(double2) * Lmax, cudaMemcpyHostToDevice);
+        G_elems = 6 * Lxyz;
     }
+    for (auto &t : tw)
+        if (t.first == Lmax) return TDDA_OK;
+    std::vector<double2> h(Lmax);
+    for (int j = 0; j < Lmax; ++j) {
+        long double ang = -2.0L * 3.141592653589793238462643383279502884L * (long double)j / Lmax;
+        h[j] = make_double2((double)cosl(ang), (double)sinl(ang));
+    }
+    double2 *d = nullptr;
+    if (cudaMalloc(&d, sizeof(double2) * Lmax) != cudaSuccess ||
+        cudaMemcpy(d, h.data(), sizeof(double2) * Lmax, cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaFree(d);
+        set_error("cannot upload twiddles");
+        return TDDA_ERR_OOM;
+    }
+    tw.emplace_back(Lmax, d);
+    return TDDA_OK;
+}
+
+const double2 *TensorScratch::twiddles(int Lmax) const {
+    for (auto &t : tw)
+        if (t.first == Lmax) return t.second;
+    return nullptr;
+}
+
+size_t TensorScratch::bytes() const {
+    return sizeof(double2) * (G_elems + (owns_tables ? (size_t)ntab : 0)) +
+           [&] { size_t b = 0; for (auto &t : tw) b += sizeof(double2) * t.first; return b; }();
+}
+
+void TensorScratch::release() {
+    cudaFree(G);
+    if (owns_tables) cudaFree(sc);
+    for (auto &t : tw) cudaFree(t.second);
+    G = nullptr;
+    sc = nullptr;
+    tw.clear();
+    G_elems = 0;
+    ntab = 0;
+}
+
+tdda_status build_tensor_async(const LatticeParams &P0, TensorScratch &ws, double2 *ahat, float2 *ahat32,
+                               cudaStream_t s, double2 *a0, cudaEvent_t ev_sums, cudaEvent_t ev_done) {
+    LatticeParams P = P0;
+    const size_t Lxyz = (size_t)P.Lx * P.Ly * P.Lz;
+    const int Lmax = lmax_of(P.Lx, P.Ly, P.Lz);
+    tdda_status st = ws.reserve(Lxyz, Lmax);
+    if (st != TDDA_OK) return st;
+    P.sc = ws.sc;
+    P.ntab = ws.ntab;
+    double2 *G = ws.G;
+    const double2 *tw = ws.twiddles(Lmax);
     cudaMemsetAsync(G, 0, sizeof(double2) * 6 * Lxyz, s);
-    cudaEventRecord(e0, s);
     const long long nent = (long long)P.nx * P.ny * P.nz;
     const long long nimg = (long long)(2 * P.MAXm + 1) * (2 * P.MAXn + 1);
     int lanes = 1;
@@ -334,7 +368,7 @@ tdda_status build_tensor(const LatticeParams &P0, const double *si, const double
     const long long threads = nent * lanes;
     count_launches(1);
     k_lattice<<<(unsigned)((threads + LNT - 1) / LNT), LNT, 0, s>>>(P, G, lanes);
-    cudaEventRecord(e1, s);
+    if (ev_sums) cudaEventRecord(ev_sums, s);
     if (a0 != nullptr)
         for (int l = 0; l < 6; ++l)
             cudaMemcpyAsync(a0 + l, G + (size_t)l * Lxyz, sizeof(double2), cudaMemcpyDeviceToHost, s);
@@ -368,13 +402,45 @@ tdda_status build_tensor(const LatticeParams &P0, const double *si, const double
     const double scale = 1.0 / ((double)P.Lx * P.Ly * P.Lz);
     count_launches(1);
     k_fold<<<1184, 256, 0, s>>>(G, P.Lx, P.Ly, P.Lz, P.Lx / 2 + 1, P.Ly / 2 + 1, P.Lz / 2 + 1, scale, ahat, ahat32);
-    cudaEventRecord(e2, s);
-    cudaError_t err = cudaStreamSynchronize(s);
-    if (err == cudaSuccess) err = cudaGetLastError();
+    if (ev_done) cudaEventRecord(ev_done, s);
+    cudaError_t err = cudaGetLastError();
     if (err != cudaSuccess) {
         set_error(std::string("tensor build: ") + cudaGetErrorString(err));
-        cleanup();
         return TDDA_ERR_CUDA;
+    }
+    return TDDA_OK;
+}
+
+tdda_status build_tensor(const LatticeParams &P, const double *si, const double *ci, long ntab,
+                         double2 *ahat, float2 *ahat32, cudaStream_t s, double *lattice_ms,
+                         double *fft_ms, double2 *a0) {
+    TensorScratch ws;
+    cudaEvent_t e0, e1, e2;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventCreate(&e2);
+    auto cleanup = [&]() {
+        ws.release();
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        cudaEventDestroy(e2);
+    };
+    tdda_status st = ws.init_tables(si, ci, ntab);
+    if (st == TDDA_OK) st = ws.reserve((size_t)P.Lx * P.Ly * P.Lz, lmax_of(P.Lx, P.Ly, P.Lz));
+    if (st != TDDA_OK) {
+        cleanup();
+        return st;
+    }
+    cudaEventRecord(e0, s);
+    st = build_tensor_async(P, ws, ahat, ahat32, s, a0, e1, e2);
+    cudaError_t err = cudaStreamSynchronize(s);
+    if (st == TDDA_OK && err != cudaSuccess) {
+        set_error(std::string("tensor build: ") + cudaGetErrorString(err));
+        st = TDDA_ERR_CUDA;
+    }
+    if (st != TDDA_OK) {
+        cleanup();
+        return st;
     }
     float a = 0, b = 0;
     cudaEventElapsedTime(&a, e0, e1);

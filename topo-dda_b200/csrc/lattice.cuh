@@ -1,6 +1,9 @@
 // Interaction-tensor assembly (lattice sums + FFT) on the device.
 #pragma once
 
+#include <utility>
+#include <vector>
+
 #include "tdda_common.cuh"
 #include "../../include/tdda.h"
 
@@ -20,6 +23,30 @@ struct LatticeParams {
     const double2 *sc;    // device (si, ci) pairs
     long ntab;
 };
+
+// Device scratch of repeated tensor builds: SiCi table, padded grid and
+// twiddle tables, kept between builds so that a build allocates nothing once
+// its sizes have been seen.  The table may be shared (owns_tables = false).
+struct TensorScratch {
+    double2 *sc = nullptr;
+    long ntab = 0;
+    bool owns_tables = false;
+    double2 *G = nullptr;
+    size_t G_elems = 0;
+    std::vector<std::pair<int, double2 *>> tw;  // (Lmax, table)
+    tdda_status init_tables(const double *si, const double *ci, long ntab);
+    tdda_status reserve(size_t Lxyz, int Lmax);
+    const double2 *twiddles(int Lmax) const;
+    size_t bytes() const;
+    void release();
+};
+
+// Enqueues one tensor build on stream s without synchronising: lattice sums
+// into ws.G, FP64 FFT, fold into ahat (and ahat32).  a0 (pinned host
+// double2[6], optional) receives the zero-offset entry once s reaches it;
+// ev_sums / ev_done (optional) are recorded after the sums and at the end.
+tdda_status build_tensor_async(const LatticeParams &P, TensorScratch &ws, double2 *ahat, float2 *ahat32,
+                               cudaStream_t s, double2 *a0, cudaEvent_t ev_sums, cudaEvent_t ev_done);
 
 // Lattice sums -> padded grid -> FP64 FFT -> folded spectral tensor
 // [hy][hx][hz][6] (scaled by 1/(Lx Ly Lz)); ahat32 optional complex64 copy.

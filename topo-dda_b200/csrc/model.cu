@@ -16,13 +16,19 @@
 #include <vector>
 
 #include "lattice.cuh"
+#include "physics.cuh"
 #include "model_view.cuh"
 #include "operator.cuh"
+#include "refine.cuh"
 
 namespace tdda {
 
 static std::atomic<long long> g_launches{0};
-void count_launches(long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+static thread_local bool g_capturing = false;
+void count_launches(long long n) {
+    if (!g_capturing) g_launches.fetch_add(n, std::memory_order_relaxed);
+}
+void set_capturing(bool on) { g_capturing = on; }
 long long launches_total() { return g_launches.load(std::memory_order_relaxed); }
 
 static thread_local std::string g_err;
@@ -32,47 +38,6 @@ const char *get_error() { return g_err.c_str(); }
 // ----------------------------------------------------------------------------
 // device helpers of the model layer
 // ----------------------------------------------------------------------------
-// polarisability of the lattice dispersion relation, 1/alpha
-// (src/Tools.cpp:353-366; interpolation src/DDAModel.cpp:319-328)
-struct AlphaParams {
-    double lam, K, d;
-    double2 m0, m1;   // rescaled materials
-    double S;         // sum_c (n_E0,c n_K,c)^2
-};
-
-__host__ __device__ inline double2 cmul_d(double2 a, double2 b) {
-    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
-}
-
-__host__ __device__ inline double2 diel_of(double rho, const AlphaParams &A) {
-    // labelfloor = floor(rho), labelnext = floor+1 unless floor >= 1
-    double lf = floor(rho);
-    double2 mf = lf >= 1.0 ? A.m1 : A.m0;
-    double2 mn = (lf >= 1.0 || lf + 1.0 >= 1.0) ? A.m1 : A.m0;
-    double w = rho - lf;
-    return make_double2(mf.x + w * (mn.x - mf.x), mf.y + w * (mn.y - mf.y));
-}
-
-__host__ __device__ inline double2 inv_alpha(double2 eps, const AlphaParams &A) {
-    // same operation order as Get_Alpha (src/Tools.cpp:353-366)
-    const double b1 = -1.891531, b2 = 0.1648469, b3 = -1.7700004;
-    const double d3 = A.d * A.d * A.d;
-    const double pre = 3.0 * d3 / (4.0 * M_PI);
-    double2 num = make_double2(pre * (eps.x - 1.0), pre * eps.y);
-    double2 a1 = cdiv(num, make_double2(eps.x + 2.0, eps.y));
-    const double kd = A.K * A.d;
-    const double kd2 = kd * kd;
-    double2 rad = make_double2(0.0, (2.0 / 3.0) * (kd * kd * kd));
-    // (b1 + eps b2 + eps b3 S) (Kd)^2 - rad
-    double2 poly = make_double2(b1 + eps.x * b2 + (eps.x * b3) * A.S, eps.y * b2 + (eps.y * b3) * A.S);
-    double2 t = make_double2(poly.x * kd2 - rad.x, poly.y * kd2 - rad.y);
-    double2 a1d = make_double2(a1.x / d3, a1.y / d3);
-    double2 res = cmul_d(a1d, t);
-    res.x = 1.0 + res.x;
-    double2 alpha = cdiv(a1, res);
-    return cdiv(make_double2(1.0, 0.0), alpha);
-}
-
 __global__ void k_alpha(long long nbox, const double *__restrict__ rho, const unsigned char *__restrict__ mask,
                         AlphaParams A, double2 *__restrict__ al, float2 *__restrict__ al32,
                         double2 *__restrict__ diel) {
@@ -214,42 +179,6 @@ __global__ void k_grad_mult(long long nbox, const double2 *__restrict__ lam, con
     }
 }
 
-// Rin[k] = sc o R[k] * scale[k] in the inner precision (scale 0 parks a
-// finished right-hand side; sc == nullptr: no Jacobi scaling)
-template <typename C>
-__global__ void k_to_inner(long long n, long long nbox, int nrhs, const double2 *__restrict__ a,
-                           const double *__restrict__ scale, const double2 *__restrict__ sc, C *__restrict__ b) {
-    long long tot = n * nrhs;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < tot; i += (long long)gridDim.x * blockDim.x) {
-        double s = scale[i / n];
-        double2 v = make_double2(a[i].x * s, a[i].y * s);
-        if (sc != nullptr) v = cmul_d(sc[(i % n) % nbox], v);
-        b[i] = from_d<C>(v);
-    }
-}
-
-// X[k] += w[k] * sc o D[k]
-template <typename C>
-__global__ void k_axpy_inner(long long n, long long nbox, int nrhs, const double *__restrict__ w,
-                             const double2 *__restrict__ sc, const C *__restrict__ d, double2 *__restrict__ x) {
-    long long tot = n * nrhs;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < tot; i += (long long)gridDim.x * blockDim.x) {
-        double s = w[i / n];
-        double2 v = to_d(d[i]);
-        if (sc != nullptr) v = cmul_d(sc[(i % n) % nbox], v);
-        x[i].x += s * v.x;
-        x[i].y += s * v.y;
-    }
-}
-
-// principal square root
-__host__ __device__ inline double2 csqrt_d(double2 z) {
-    double r = hypot(z.x, z.y);
-    double re = sqrt(0.5 * (r + z.x));
-    double im = sqrt(0.5 * fmax(r - z.x, 0.0));
-    return make_double2(re, z.y < 0 ? -im : im);
-}
-
 // Jacobi scaling of the operator A + diag(al): D = al + a0 (a0: mean of the
 // diagonal of the zero-offset lattice entry), sc = D^(-1/2), alS = sc^2 al.
 __global__ void k_jacobi(long long nbox, const double2 *__restrict__ al, const unsigned char *__restrict__ mask,
@@ -257,10 +186,7 @@ __global__ void k_jacobi(long long nbox, const double2 *__restrict__ al, const u
                          float2 *__restrict__ sc32, float2 *__restrict__ alS32) {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nbox; i += (long long)gridDim.x * blockDim.x) {
         double2 s = make_double2(1.0, 0.0), a = al[i];
-        if (mask == nullptr || mask[i] != 0) {
-            double2 d = make_double2(a.x + a0.x, a.y + a0.y);
-            s = cdiv(make_double2(1.0, 0.0), csqrt_d(d));
-        }
+        if (mask == nullptr || mask[i] != 0) s = jacobi_scale(a, a0);
         double2 as = cmul_d(cmul_d(s, s), a);
         sc[i] = s;
         alS[i] = as;
@@ -271,17 +197,6 @@ __global__ void k_jacobi(long long nbox, const double2 *__restrict__ al, const u
     }
 }
 
-// d(1/alpha)/d rho: (-3 / (c (eps - 1)^2) + (b2 + b3 S) K^2 / d) (m1 - m0),
-// c = 3 d^3 / (4 pi) -- the closed-form derivative of Get_Alpha's inverse.
-__host__ __device__ inline double2 dal_drho(double2 eps, const AlphaParams &A) {
-    const double b2 = 0.1648469, b3 = -1.7700004;
-    const double c = 3.0 * A.d * A.d * A.d / (4.0 * M_PI);
-    double2 em1 = make_double2(eps.x - 1.0, eps.y);
-    double2 sq = cmul_d(em1, em1);
-    double2 t = cdiv(make_double2(-3.0 / c, 0.0), sq);
-    t.x += (b2 + b3 * A.S) * A.K * A.K / A.d;
-    return cmul_d(t, make_double2(A.m1.x - A.m0.x, A.m1.y - A.m0.y));
-}
 
 // adjoint right-hand side dJ/dx - i dJ/dy of J = log S, S = sum |al P|^q:
 // q |al|^q |P|^(q-2) conj(P) / S
@@ -702,117 +617,39 @@ static tdda_status update_alpha(tdda_model *m) {
 static tdda_status solve_c128(tdda_model *m, const double2 *B, double2 *X, int nrhs, bool x0_zero,
                               int max_iter, double tol, tdda_solve_info *info) {
     TRY(ensure_krylov(m, nrhs));
-    return bicgstab_device<double2>(m->op, m->kv, m->al, B, X, nrhs, x0_zero, max_iter, tol, m->stream, info,
-                                    nullptr, 0, nullptr);
+    return bicgstab_device<double2>(m->op, m->kv, m->al, nullptr, B, X, nrhs, x0_zero, max_iter, tol, m->stream,
+                                    info, KrylovOptions{});
 }
 
-// Inner-solve workspace of the refinement driver, per inner precision.
-template <typename C> struct Inner {
-    ConvOperator<C> *op;
-    Krylov<C> *kv;
-    const C *al;  // al, or sc^2 al under Jacobi scaling
-    const C *sc;  // Jacobi scale or nullptr
-    C *R, *D;
-};
-
-static Inner<float2> inner_of(tdda_model *m, float2 *) {
+// Refinement workspace of the model, per inner precision.
+static RefineWork<float2> refine_work(tdda_model *m, float2 *) {
     const bool j = m->precond != 0;
-    return {&m->op32, &m->kv32, j ? m->alS32 : m->al32, j ? m->sc32 : nullptr, m->R32, m->D32};
+    RefineWork<float2> w;
+    w.op = &m->op32; w.kv = &m->kv32; w.al = j ? m->alS32 : m->al32; w.sc = j ? m->sc32 : nullptr;
+    w.R = m->R32; w.D = m->D32;
+    return w;
 }
 
-static Inner<double2> inner_of(tdda_model *m, double2 *) {
+static RefineWork<double2> refine_work(tdda_model *m, double2 *) {
     const bool j = m->precond != 0;
-    return {&m->op, &m->kv, j ? m->alS64 : m->al, j ? m->sc64 : nullptr, m->R64, m->D64};
+    RefineWork<double2> w;
+    w.op = &m->op; w.kv = &m->kv; w.al = j ? m->alS64 : m->al; w.sc = j ? m->sc64 : nullptr;
+    w.R = m->R64; w.D = m->D64;
+    return w;
 }
 
-// Iterative refinement: the residual R = B - A X and the accumulation of X are
-// complex128; each correction solves A D = R / ||R|| with BiCGSTAB in the inner
-// precision C (complex64 for mixed precision), optionally Jacobi-scaled, until
-// the TRUE residual ||B - A X|| / ||B|| <= tol.
+// Iterative refinement on the complex128 residual with inner solves in C
+// (complex64 for mixed precision), Jacobi-scaled when precond is on.
 template <typename C>
 static tdda_status solve_refined(tdda_model *m, const double2 *B, double2 *X, int nrhs, bool x0_zero,
                                  int max_iter, double tol, tdda_solve_info *info) {
     TRY(ensure_refine(m, nrhs, (C *)nullptr));
-    Inner<C> in = inner_of(m, (C *)nullptr);
-    const bool single = sizeof(C) == sizeof(float2);
-    const long long n = 3 * m->nbox;
-    if (x0_zero) TDDA_CUDA_TRY(cudaMemsetAsync(X, 0, sizeof(double2) * n * nrhs, m->stream));
-    std::vector<int> done(nrhs, 0), refine(nrhs, 0), inner(nrhs, 0);
-    std::vector<double> err(nrhs, 0.0);
-    std::vector<int> status(nrhs, TDDA_SOLVE_RUNNING), slow(nrhs, 0);
-    std::vector<double> prev(nrhs, 1e300);
-    const int max_refine = 12;
-    // an inner complex64 solve that has not cut its residual by 10% in this many
-    // iterations has reached what single precision can give; refinement takes over
-    const int kInnerStall = 150;
-    for (int outer = 0; outer <= max_refine; ++outer) {
-        TRY(residual_c128(m->op, m->al, B, X, m->Rm, m->st_res, nrhs, m->stream));
-        TDDA_CUDA_TRY(cudaMemcpyAsync(m->st_res_host, m->st_res, sizeof(SolverState) * nrhs, cudaMemcpyDeviceToHost, m->stream));
-        TDDA_CUDA_TRY(cudaStreamSynchronize(m->stream));
-        bool all = true;
-        for (int k = 0; k < nrhs; ++k) {
-            if (done[k]) continue;
-            const SolverState &S = m->st_res_host[k];
-            err[k] = S.err;
-            if (S.enorm == 0.0) {
-                TDDA_CUDA_TRY(cudaMemsetAsync(X + (size_t)k * n, 0, sizeof(double2) * n, m->stream));
-                done[k] = 1; status[k] = TDDA_SOLVE_ZERO_RHS; err[k] = 0.0;
-            } else if (S.err <= tol) {
-                done[k] = 1; status[k] = TDDA_SOLVE_CONVERGED;
-            } else if (!std::isfinite(S.err)) {
-                done[k] = 1; status[k] = TDDA_SOLVE_NONFINITE;
-            } else if (outer == max_refine || inner[k] >= max_iter) {
-                done[k] = 1; status[k] = TDDA_SOLVE_MAXITER;
-            } else {
-                // two refinements in a row that do not halve the true residual: stop
-                slow[k] = (S.err > 0.5 * prev[k]) ? slow[k] + 1 : 0;
-                if (slow[k] >= 2) { done[k] = 1; status[k] = TDDA_SOLVE_STAGNATED; }
-            }
-            prev[k] = S.err;
-            all &= (done[k] != 0);
-        }
-        if (all) break;
-        // one batched complex64 solve over every unfinished right-hand side,
-        // each normalised by its own residual norm (finished ones get a zero RHS)
-        std::vector<double> h(3 * (size_t)nrhs, 0.0);
-        int budget = 1;
-        for (int k = 0; k < nrhs; ++k) {
-            if (done[k]) continue;
-            const SolverState &S = m->st_res_host[k];
-            const double rn = S.err * S.enorm;
-            h[k] = 1.0 / rn;                                   // scale into the inner RHS
-            h[nrhs + k] = rn;                                  // scale of the correction
-            // inner tolerance: what this step must gain, floored where single
-            // precision stops paying off
-            h[2 * nrhs + k] = std::max(0.5 * tol / S.err, single ? 2e-6 : 0.0);
-            budget = std::max(budget, max_iter - inner[k]);
-        }
-        TDDA_CUDA_TRY(cudaMemcpyAsync(m->d_part, h.data(), sizeof(double) * 3 * nrhs, cudaMemcpyHostToDevice, m->stream));
-        const double2 *sc = m->precond ? m->sc64 : nullptr;
-        count_launches(1);
-        k_to_inner<C><<<grid_for(n * nrhs), 256, 0, m->stream>>>(n, m->nbox, nrhs, m->Rm, m->d_part, sc, in.R);
-        std::vector<tdda_solve_info> ii(nrhs);
-        TRY(bicgstab_device<C>(*in.op, *in.kv, in.al, in.R, in.D, nrhs, true, budget, h[2 * nrhs], m->stream,
-                               ii.data(), h.data() + 2 * nrhs, kInnerStall, in.sc));
-        count_launches(1);
-        k_axpy_inner<C><<<grid_for(n * nrhs), 256, 0, m->stream>>>(n, m->nbox, nrhs, m->d_part + nrhs, sc, in.D, X);
-        TDDA_CUDA_TRY(cudaGetLastError());
-        for (int k = 0; k < nrhs; ++k) {
-            if (done[k]) continue;
-            inner[k] += ii[k].iterations;
-            refine[k] += 1;
-        }
-    }
-    if (info)
-        for (int k = 0; k < nrhs; ++k) {
-            info[k].iterations = inner[k];
-            info[k].error = err[k];
-            info[k].status = status[k];
-            info[k].refinements = refine[k];
-            info[k].inner_iterations = inner[k];
-            info[k].true_error = err[k];
-        }
-    return TDDA_OK;
+    RefineWork<C> w = refine_work(m, (C *)nullptr);
+    w.op64 = &m->op; w.al64 = m->al; w.sc64 = m->precond ? m->sc64 : nullptr;
+    w.Rm = m->Rm; w.st_res = m->st_res; w.st_res_host = m->st_res_host;
+    w.d_part = m->d_part; w.h_part = m->h_part;
+    w.nbox = m->nbox; w.s = m->stream;
+    return refine_solve<C>(w, B, X, nrhs, x0_zero, max_iter, tol, info);
 }
 
 static tdda_status solve_internal(tdda_model *m, const double2 *B, double2 *X, int nrhs, bool x0_zero,
@@ -1224,12 +1061,10 @@ tdda_status tdda_matvec_c64(tdda_model *m, const double *x, double *y, int with_
     TRY(to_internal(m, x, m->bufB, 1));
     const double one = 1.0;
     TDDA_CUDA_TRY(cudaMemcpyAsync(m->d_part, &one, sizeof(double), cudaMemcpyHostToDevice, m->stream));
-    count_launches(1);
-    k_to_inner<float2><<<grid_for(n), 256, 0, m->stream>>>(n, m->nbox, 1, m->bufB, m->d_part, nullptr, m->R32);
+    launch_to_inner<float2>(n, m->nbox, 1, 0, m->bufB, m->d_part, nullptr, m->R32, m->stream);
     TRY(m->op32.apply(m->R32, m->D32, with_al ? m->al32 : nullptr, 1, m->stream));
     TDDA_CUDA_TRY(cudaMemsetAsync(m->bufX, 0, sizeof(double2) * n, m->stream));
-    count_launches(1);
-    k_axpy_inner<float2><<<grid_for(n), 256, 0, m->stream>>>(n, m->nbox, 1, m->d_part, nullptr, m->D32, m->bufX);
+    launch_axpy_inner<float2>(n, m->nbox, 1, 0, m->d_part, nullptr, m->D32, m->bufX, m->stream);
     TDDA_CUDA_TRY(cudaGetLastError());
     return to_host(m, m->bufX, y, 1);
 }

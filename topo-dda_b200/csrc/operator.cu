@@ -419,14 +419,23 @@ __global__ void __launch_bounds__(NT) k_inv_yz(ConvGeom g, const C *__restrict__
 // Optional diagonal (Jacobi) scaling: with sc = D^(-1/2) per cell the passes
 // apply S A S + diag(alS) (alS = sc^2 al) instead of A + diag(al): pass 1
 // scales what it transforms, pass 3 scales the convolution.  sc == nullptr is
-// the unscaled operator of the reference.
+// the unscaled operator of the reference.  The diagonal (al, sc) is shared by
+// every right-hand side (dstride = 0) or held per right-hand side at
+// [rhs][cell] (dstride = nbox): the polarisabilities of one structure differ
+// between incident polarisations (src/Tools.cpp:353-366 depends on n_E0).
 template <typename C> struct VecBase {
     long long nbox;
     const C *sc = nullptr;
+    size_t dstride = 0;
     __device__ __forceinline__ size_t idx(int rhs, int c, long long cell) const {
         return ((size_t)rhs * 3 + c) * (size_t)nbox + (size_t)cell;
     }
-    __device__ __forceinline__ C scaled(long long cell, C v) const { return sc != nullptr ? sc[cell] * v : v; }
+    __device__ __forceinline__ size_t didx(int rhs, long long cell) const {
+        return (size_t)rhs * dstride + (size_t)cell;
+    }
+    __device__ __forceinline__ C scaled(int rhs, long long cell, C v) const {
+        return sc != nullptr ? sc[didx(rhs, cell)] * v : v;
+    }
 };
 
 template <typename C> struct ProLoad : VecBase<C> {
@@ -434,7 +443,7 @@ template <typename C> struct ProLoad : VecBase<C> {
     const SolverState *st;  // optional
     __device__ bool skip(int rhs) const { return st != nullptr && st[rhs].done; }
     __device__ C load(int rhs, int c, long long cell) const {
-        return this->scaled(cell, x[this->idx(rhs, c, cell)]);
+        return this->scaled(rhs, cell, x[this->idx(rhs, c, cell)]);
     }
 };
 
@@ -454,7 +463,7 @@ template <typename C> struct ProP : VecBase<C> {
             v = v + beta * (p[i] - zeta * Ap[i]);
         }
         p[i] = v;
-        return this->scaled(cell, v);
+        return this->scaled(rhs, cell, v);
     }
 };
 
@@ -470,7 +479,7 @@ template <typename C> struct ProT : VecBase<C> {
         C alpha = from_d<C>(st[rhs].alpha);
         C v = r[i] - alpha * Ap[i];
         t[i] = v;
-        return this->scaled(cell, v);
+        return this->scaled(rhs, cell, v);
     }
 };
 
@@ -479,9 +488,9 @@ template <typename C> struct EpiBase : VecBase<C> {
     double2 *part;
     unsigned *counter;
     size_t pstride;
-    __device__ __forceinline__ C masked(long long cell, C conv) const {
+    __device__ __forceinline__ C masked(int rhs, long long cell, C conv) const {
         if (mask != nullptr && mask[cell] == 0) return czero<C>();
-        return this->scaled(cell, conv);
+        return this->scaled(rhs, cell, conv);
     }
 };
 
@@ -494,8 +503,8 @@ template <typename C> struct EpiMatvec : EpiBase<C> {
     __device__ bool skip(int) const { return false; }
     __device__ void apply(int rhs, int c, long long cell, C conv, double2 *) const {
         size_t i = this->idx(rhs, c, cell);
-        C v = this->masked(cell, conv);
-        if (al != nullptr) v = v + al[cell] * x[i];
+        C v = this->masked(rhs, cell, conv);
+        if (al != nullptr) v = v + al[this->didx(rhs, cell)] * x[i];
         y[i] = v;
     }
     __device__ void operator()(int, const double2 *) const {}
@@ -510,7 +519,7 @@ template <typename C> struct EpiInit : EpiBase<C> {
     __device__ bool skip(int rhs) const { return false; }
     __device__ void apply(int rhs, int c, long long cell, C conv, double2 *acc) const {
         size_t i = this->idx(rhs, c, cell);
-        C ax = this->masked(cell, conv) + al[cell] * x0[i];
+        C ax = this->masked(rhs, cell, conv) + al[this->didx(rhs, cell)] * x0[i];
         C bb = b[i];
         C v = bb - ax;
         r[i] = v;
@@ -545,7 +554,7 @@ template <typename C> struct EpiAp : EpiBase<C> {
     __device__ bool skip(int rhs) const { return st[rhs].done; }
     __device__ void apply(int rhs, int c, long long cell, C conv, double2 *acc) const {
         size_t i = this->idx(rhs, c, cell);
-        C v = this->masked(cell, conv) + al[cell] * p[i];
+        C v = this->masked(rhs, cell, conv) + al[this->didx(rhs, cell)] * p[i];
         Ap[i] = v;
         double2 d = cdot1(to_d(r0[i]), to_d(v));
         acc[0].x += d.x;
@@ -567,7 +576,7 @@ template <typename C> struct EpiAt : EpiBase<C> {
     __device__ void apply(int rhs, int c, long long cell, C conv, double2 *acc) const {
         size_t i = this->idx(rhs, c, cell);
         C tv = t[i];
-        C v = this->masked(cell, conv) + al[cell] * tv;
+        C v = this->masked(rhs, cell, conv) + al[this->didx(rhs, cell)] * tv;
         At[i] = v;
         double2 vd = to_d(v);
         double2 d = cdot1(vd, to_d(tv));
@@ -815,6 +824,20 @@ template <typename C> tdda_status ConvOperator<C>::init(int nx, int ny, int nz, 
     return TDDA_OK;
 }
 
+size_t conv_workspace_bytes(int nx, int ny, int nz, int nrhs_cap, int esize) {
+    ConvGeom g;
+    std::string why;
+    if (!plan_geom(nx, ny, nz, 1, esize, g, why)) return 0;
+    const size_t partial_cap = (size_t)std::max(3 * nx, UPD_BLOCKS) * 2;
+    return (size_t)esize * g.Lmax + (size_t)esize * nrhs_cap * 3 * g.tcomp + sizeof(double2) * partial_cap * nrhs_cap +
+           sizeof(unsigned) * nrhs_cap;
+}
+
+bool conv_supported(int nx, int ny, int nz, int nrhs, int esize, std::string &why) {
+    ConvGeom g;
+    return plan_geom(nx, ny, nz, nrhs, esize, g, why);
+}
+
 template <typename C> void ConvOperator<C>::release() {
     cudaFree(ahat); cudaFree(tw); cudaFree(T); cudaFree(partials); cudaFree(counters);
     ahat = nullptr; tw = nullptr; T = nullptr; partials = nullptr; counters = nullptr;
@@ -896,9 +919,9 @@ template <typename C> void Krylov<C>::release() {
 }
 
 template <typename C>
-tdda_status bicgstab_device(ConvOperator<C> &op, Krylov<C> &kv, const C *al, const C *B, C *X,
+tdda_status bicgstab_device(ConvOperator<C> &op, Krylov<C> &kv, const C *al, const C *sc, const C *B, C *X,
                             int nrhs, bool x0_zero, int max_iter, double tol, cudaStream_t s,
-                            tdda_solve_info *info, const double *tols, int stall_limit, const C *sc) {
+                            tdda_solve_info *info, const KrylovOptions &o) {
     if (nrhs > kv.nrhs || nrhs > op.nrhs_cap) { set_error("nrhs exceeds workspace"); return TDDA_ERR_BAD_ARG; }
     ConvGeom g;
     if (!geom_for(op, nrhs, g)) { set_error("batch does not fit the x pass"); return TDDA_ERR_UNSUPPORTED; }
@@ -908,8 +931,8 @@ tdda_status bicgstab_device(ConvOperator<C> &op, Krylov<C> &kv, const C *al, con
         std::memset(&S, 0, sizeof(S));
         S.it = -1;
         S.max_iter = max_iter;
-        S.tol = tols != nullptr ? tols[k] : tol;
-        S.stall_limit = stall_limit;
+        S.tol = o.tols != nullptr ? o.tols[k] : tol;
+        S.stall_limit = o.stall_limit;
         S.best_it = 0;
         S.best_err = 1e300;
         S.status = TDDA_SOLVE_RUNNING;
@@ -922,47 +945,84 @@ tdda_status bicgstab_device(ConvOperator<C> &op, Krylov<C> &kv, const C *al, con
         k_init_zero<C><<<gi, NT, 0, s>>>(n, B, X, kv.r, kv.r0, kv.st, op.partials, op.counters, ps);
     } else {
         ProLoad<C> pro{};
-        pro.nbox = g.nbox; pro.x = X; pro.st = nullptr; pro.sc = sc;
+        pro.nbox = g.nbox; pro.x = X; pro.st = nullptr; pro.sc = sc; pro.dstride = o.dstride;
         EpiInit<C> epi{};
         epi.nbox = g.nbox; epi.mask = op.mask; epi.part = op.partials; epi.counter = op.counters;
         epi.pstride = ps; epi.x0 = X; epi.b = B; epi.al = al; epi.r = kv.r; epi.r0 = kv.r0; epi.st = kv.st;
-        epi.sc = sc;
+        epi.sc = sc; epi.dstride = o.dstride;
         run_conv(op, g, nrhs, pro, epi, nullptr, s);
     }
     TDDA_CUDA_TRY(cudaGetLastError());
 
-    // one BiCGSTAB step: Ap, alpha, t, At, zeta, P/r update, beta
+    // one BiCGSTAB step: Ap, alpha, t, At, zeta, P/r update, beta (7 launches)
+    constexpr int kLaunchesPerStep = 7;
     auto step = [&](bool first) {
         ProP<C> pp{};
         pp.nbox = g.nbox; pp.r = kv.r; pp.p = kv.p; pp.Ap = kv.Ap; pp.st = kv.st; pp.first = first ? 1 : 0;
+        pp.sc = sc; pp.dstride = o.dstride;
         EpiAp<C> ea{};
         ea.nbox = g.nbox; ea.mask = op.mask; ea.part = op.partials; ea.counter = op.counters; ea.pstride = ps;
         ea.p = kv.p; ea.al = al; ea.r0 = kv.r0; ea.Ap = kv.Ap; ea.st = kv.st;
-        pp.sc = sc;
-        ea.sc = sc;
+        ea.sc = sc; ea.dstride = o.dstride;
         run_conv(op, g, nrhs, pp, ea, kv.st, s);
         ProT<C> pt{};
         pt.nbox = g.nbox; pt.r = kv.r; pt.Ap = kv.Ap; pt.t = kv.t; pt.st = kv.st;
+        pt.sc = sc; pt.dstride = o.dstride;
         EpiAt<C> et{};
         et.nbox = g.nbox; et.mask = op.mask; et.part = op.partials; et.counter = op.counters; et.pstride = ps;
         et.t = kv.t; et.al = al; et.At = kv.At; et.st = kv.st;
-        pt.sc = sc;
-        et.sc = sc;
+        et.sc = sc; et.dstride = o.dstride;
         run_conv(op, g, nrhs, pt, et, kv.st, s);
         dim3 gu(UPD_BLOCKS, nrhs);
         count_launches(1);
         k_update<C><<<gu, NT, 0, s>>>(n, X, kv.p, kv.t, kv.At, kv.r, kv.r0, kv.st, op.partials, op.counters, ps);
     };
 
+    // Optional CUDA graph of graph_steps consecutive iterations, replayed
+    // between polls: every launch reads its scalars from the device states and
+    // returns at once for a finished right-hand side, so a replay past
+    // convergence is harmless.
+    cudaGraphExec_t exec = nullptr;
+    struct GraphGuard {
+        cudaGraphExec_t *e;
+        ~GraphGuard() { if (*e) cudaGraphExecDestroy(*e); }
+    } guard{&exec};
+    auto capture = [&]() -> tdda_status {
+        cudaGraph_t graph = nullptr;
+        set_capturing(true);
+        cudaError_t err = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+        if (err == cudaSuccess) {
+            for (int k = 0; k < o.graph_steps; ++k) step(false);
+            err = cudaStreamEndCapture(s, &graph);
+        }
+        set_capturing(false);
+        if (err == cudaSuccess) err = cudaGraphInstantiate(&exec, graph, 0);
+        if (graph) cudaGraphDestroy(graph);
+        if (err != cudaSuccess) {
+            set_error(std::string("graph capture: ") + cudaGetErrorString(err));
+            return TDDA_ERR_CUDA;
+        }
+        return TDDA_OK;
+    };
+
     long long launched = 0;
     bool first = true;
     int chunk = 2;
     for (;;) {
-        for (int k = 0; k < chunk; ++k) {
-            step(first);
-            first = false;
+        if (o.graph_steps > 0 && !first) {
+            if (exec == nullptr) { tdda_status st = capture(); if (st != TDDA_OK) return st; }
+            const int reps = std::max(1, chunk / o.graph_steps);
+            for (int k = 0; k < reps; ++k) TDDA_CUDA_TRY(cudaGraphLaunch(exec, s));
+            count_launches((long long)reps * o.graph_steps * kLaunchesPerStep);
+            launched += (long long)reps * o.graph_steps;
+        } else {
+            const int steps = (o.graph_steps > 0) ? 1 : chunk;  // the first step sets p = r
+            for (int k = 0; k < steps; ++k) {
+                step(first);
+                first = false;
+            }
+            launched += steps;
         }
-        launched += chunk;
         TDDA_CUDA_TRY(cudaGetLastError());
         TDDA_CUDA_TRY(cudaMemcpyAsync(kv.st_host, kv.st, sizeof(SolverState) * nrhs, cudaMemcpyDeviceToHost, s));
         TDDA_CUDA_TRY(cudaStreamSynchronize(s));
@@ -993,13 +1053,11 @@ template struct ConvOperator<float2>;
 template struct Krylov<double2>;
 template struct Krylov<float2>;
 template tdda_status bicgstab_device<double2>(ConvOperator<double2> &, Krylov<double2> &, const double2 *,
-                                              const double2 *, double2 *, int, bool, int, double,
-                                              cudaStream_t, tdda_solve_info *, const double *, int,
-                                              const double2 *);
+                                              const double2 *, const double2 *, double2 *, int, bool, int, double,
+                                              cudaStream_t, tdda_solve_info *, const KrylovOptions &);
 template tdda_status bicgstab_device<float2>(ConvOperator<float2> &, Krylov<float2> &, const float2 *,
-                                             const float2 *, float2 *, int, bool, int, double,
-                                             cudaStream_t, tdda_solve_info *, const double *, int,
-                                             const float2 *);
+                                             const float2 *, const float2 *, float2 *, int, bool, int, double,
+                                             cudaStream_t, tdda_solve_info *, const KrylovOptions &);
 
 template <typename C>
 tdda_status profile_apply(ConvOperator<C> &op, const C *x, C *y, const C *al, int nrhs, int iters,
@@ -1053,7 +1111,7 @@ template tdda_status profile_apply<float2>(ConvOperator<float2> &, const float2 
                                            int, cudaStream_t, double *, double *);
 
 tdda_status residual_c128(ConvOperator<double2> &op, const double2 *al, const double2 *B, const double2 *X,
-                          double2 *R, SolverState *st, int nrhs, cudaStream_t s) {
+                          double2 *R, SolverState *st, int nrhs, cudaStream_t s, size_t dstride) {
     ConvGeom g;
     if (nrhs > op.nrhs_cap || !geom_for(op, nrhs, g)) { set_error("batch does not fit"); return TDDA_ERR_UNSUPPORTED; }
     ProLoad<double2> pro{};
@@ -1061,6 +1119,7 @@ tdda_status residual_c128(ConvOperator<double2> &op, const double2 *al, const do
     EpiInit<double2> epi{};
     epi.nbox = g.nbox; epi.mask = op.mask; epi.part = op.partials; epi.counter = op.counters;
     epi.pstride = (size_t)op.partial_cap; epi.x0 = X; epi.b = B; epi.al = al; epi.r = R; epi.r0 = R; epi.st = st;
+    epi.dstride = dstride;
     run_conv(op, g, nrhs, pro, epi, nullptr, s);
     TDDA_CUDA_TRY(cudaGetLastError());
     return TDDA_OK;

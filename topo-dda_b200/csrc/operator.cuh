@@ -43,6 +43,12 @@ template <typename C> struct ConvOperator {
     tdda_status apply(const C *x, C *y, const C *al, int nrhs, cudaStream_t s);
 };
 
+// Device bytes ConvOperator<C>::init allocates (twiddles, spectral
+// intermediate, reduction scratch; not the tensor) for esize = sizeof(C).
+size_t conv_workspace_bytes(int nx, int ny, int nz, int nrhs_cap, int esize);
+// Whether the fused operator supports this grid with nrhs right-hand sides.
+bool conv_supported(int nx, int ny, int nz, int nrhs, int esize, std::string &why);
+
 // Vectors of one BiCGSTAB instance ([nrhs][3][nbox] each) + states.
 template <typename C> struct Krylov {
     int nrhs = 0;
@@ -54,16 +60,24 @@ template <typename C> struct Krylov {
     void release();
 };
 
+// Options of the device BiCGSTAB driver.
+struct KrylovOptions {
+    const double *tols = nullptr;  // tolerance per right-hand side (host), or nullptr: one tol for all
+    int stall_limit = 0;           // 0: off (reference semantics); else stop after this many
+                                   // iterations without a 10% drop of the residual
+    size_t dstride = 0;            // diagonal (al, sc) per rhs at [rhs][cell] when nbox, shared when 0
+    int graph_steps = 0;           // > 0: capture this many iterations in a CUDA graph and replay it
+};
+
 // BiCGSTAB of DDAModel::bicgstab on the fused operator: solves
 // (A + diag(al)) X = B for nrhs right-hand sides, X holds the initial guess
-// (nullptr-equivalent zero when x0_zero).  Runs fully on the device; the host
-// polls the done flags once per chunk of iterations.
+// (zero when x0_zero).  With sc (Jacobi scale per cell) the operator is
+// S A S + diag(al) and al must already be sc^2 al.  Runs fully on the device;
+// the host polls the done flags once per chunk of iterations.
 template <typename C>
-tdda_status bicgstab_device(ConvOperator<C> &op, Krylov<C> &kv, const C *al, const C *B, C *X,
+tdda_status bicgstab_device(ConvOperator<C> &op, Krylov<C> &kv, const C *al, const C *sc, const C *B, C *X,
                             int nrhs, bool x0_zero, int max_iter, double tol, cudaStream_t s,
-                            tdda_solve_info *info, const double *tols /* per rhs, or nullptr */,
-                            int stall_limit /* 0: off (reference semantics) */,
-                            const C *sc /* Jacobi scale per cell (al must then be sc^2 al), or nullptr */);
+                            tdda_solve_info *info, const KrylovOptions &opts);
 
 // One operator application for one right-hand side whose spectral
 // intermediate lives in T_ext (3 * g.tcomp elements) instead of op.T.
@@ -74,7 +88,7 @@ tdda_status apply_external_scratch(const ConvOperator<C> &op, C *T_ext, const C 
 // R = B - (A + diag al) X in complex128 (one fused convolution); st receives
 // enorm = ||B|| and err = ||R|| / ||B|| per right-hand side.
 tdda_status residual_c128(ConvOperator<double2> &op, const double2 *al, const double2 *B, const double2 *X,
-                          double2 *R, SolverState *st, int nrhs, cudaStream_t s);
+                          double2 *R, SolverState *st, int nrhs, cudaStream_t s, size_t dstride = 0);
 
 // Times `iters` back-to-back applications of the operator, then each pass
 // alone, with CUDA events on stream s: ms_total = mean per application,

@@ -101,6 +101,8 @@ int next_fft_len(int minlen);   // smallest 2^a 3^b >= minlen
 
 // number of kernels this library has launched (all devices, all models)
 void count_launches(long long n);
+// while a CUDA graph is being captured on this thread its launches are counted at replay
+void set_capturing(bool on);
 long long launches_total();
 
 // error state (thread-local message for tdda_last_error)

@@ -84,6 +84,59 @@ class ModelInfo(ctypes.Structure):
     ]
 
 
+MAX_POL = 4  # TDDA_SERVER_MAX_POL
+
+
+class ServerConfig(ctypes.Structure):
+    _fields_ = [
+        ("hbm_budget_bytes", ctypes.c_int64), ("workers", ctypes.c_int32), ("max_rhs", ctypes.c_int32),
+        ("use_graphs", ctypes.c_int32), ("graph_steps", ctypes.c_int32),
+    ]
+
+
+class Request(ctypes.Structure):
+    _fields_ = [
+        ("num_x", ctypes.c_int32), ("num_y", ctypes.c_int32), ("num_z", ctypes.c_int32),
+        ("d", ctypes.c_double), ("lam", ctypes.c_double), ("nback", ctypes.c_double), ("E0", ctypes.c_double),
+        ("material", ctypes.c_double * 4),
+        ("MAXm", ctypes.c_int32), ("MAXn", ctypes.c_int32),
+        ("Lm", ctypes.c_double), ("Ln", ctypes.c_double),
+        ("method", ctypes.c_int32),
+        ("n_K", ctypes.c_double * 3),
+        ("npol", ctypes.c_int32),
+        ("n_E0", (ctypes.c_double * 3) * MAX_POL),
+        ("rho", _dp),
+        ("precision", ctypes.c_int32),
+        ("tol", ctypes.c_double),
+        ("max_iter", ctypes.c_int32),
+        ("P_out", _dp), ("E_out", _dp),
+    ]
+
+
+class RequestResult(ctypes.Structure):
+    _fields_ = [
+        ("status", ctypes.c_int32),
+        ("info", SolveInfo * MAX_POL),
+        ("batch_rhs", ctypes.c_int32), ("batch_requests", ctypes.c_int32), ("cache_hit", ctypes.c_int32),
+        ("worker", ctypes.c_int32),
+        ("queue_ms", ctypes.c_double), ("build_ms", ctypes.c_double), ("solve_ms", ctypes.c_double),
+        ("total_ms", ctypes.c_double),
+    ]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [
+        ("submitted", ctypes.c_int64), ("completed", ctypes.c_int64), ("failed", ctypes.c_int64),
+        ("cache_hits", ctypes.c_int64), ("cache_misses", ctypes.c_int64), ("evictions", ctypes.c_int64),
+        ("batches", ctypes.c_int64), ("merged_requests", ctypes.c_int64),
+        ("bytes_in_use", ctypes.c_int64), ("peak_bytes", ctypes.c_int64), ("cached_tensors", ctypes.c_int64),
+        ("max_concurrent", ctypes.c_int32), ("admission_waits", ctypes.c_int32),
+    ]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 # every symbol include/tdda.h declares, with its ctypes signature
 SIGNATURES = {
     "tdda_status_string": (ctypes.c_char_p, [ctypes.c_int]),
@@ -125,6 +178,13 @@ SIGNATURES = {
                                            ctypes.POINTER(SolveInfo)]),
     "tdda_matvec_device_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                                   ctypes.c_int, ctypes.c_void_p]),
+    "tdda_server_create": (ctypes.c_int, [ctypes.POINTER(ServerConfig), _dp, _dp, ctypes.c_int64,
+                                          ctypes.POINTER(ctypes.c_void_p)]),
+    "tdda_server_submit": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_int64)]),
+    "tdda_server_wait": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_double,
+                                        ctypes.POINTER(RequestResult)]),
+    "tdda_server_get_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ServerStats)]),
+    "tdda_server_destroy": (None, [ctypes.c_void_p]),
 }
 
 _lib = None
