@@ -212,9 +212,12 @@ tdda_status tdda_matvec_device_noalloc(tdda_model *m, const void *x_dev, void *y
  *   - the FFT'd interaction tensor of each (grid, d, lambda, nback, period,
  *     method) stays resident and is reused by later requests with the same key;
  *     idle tensors are evicted least-recently-used when the budget is short;
- *   - queued requests with the same key are merged with the admitted one into
- *     one multi-right-hand-side solve (each polarisation is a right-hand side
- *     with its own polarisability), up to max_rhs right-hand sides;
+ *   - queued requests of the same grid (and precision, tolerance, iteration
+ *     limit) are merged with the admitted one into one multi-right-hand-side
+ *     solve: each polarisation is a right-hand side with its own
+ *     polarisability and its own request's tensor (shared when keys match), up
+ *     to max_rhs right-hand sides or fewer where the grid's x pass cannot hold
+ *     that many;
  *   - each worker drives its batches on its own CUDA stream, so batches of
  *     different workers overlap on the device; BiCGSTAB iterations are replayed
  *     from CUDA graphs when use_graphs is set.

@@ -59,9 +59,11 @@ def test_matvec_matches_oracle(sici, shape, periodic, method):
 
 
 @pytest.mark.parametrize("shape,periodic", [((64, 64, 16), 1), ((128, 128, 32), 1), ((48, 40, 12), 0),
-                                            ((16, 16, 8), 2), ((32, 32, 8), 0)])
+                                            ((16, 16, 8), 2), ((32, 32, 8), 0), ((48, 48, 12), 0),
+                                            ((96, 96, 16), 0), ((96, 96, 24), 1)])
 def test_matvec_large_grids(sici, shape, periodic):
-    """FFT lengths 128/256/96/80/24 (the benchmark grids), complex128 and complex64."""
+    """FFT lengths 128/256/96/80/24/192/48 (the benchmark and serving grids),
+    complex128 and complex64."""
     from dda_model import DDAModel
     from oracle.dda_oracle import OracleModel
 
@@ -249,7 +251,7 @@ def test_mixed_precision_batched_rhs(sici):
 
 
 @pytest.mark.parametrize("shape,nrhs", [((16, 16, 8), 2), ((16, 16, 8), 3), ((32, 32, 16), 2), ((64, 64, 16), 2),
-                                        ((128, 128, 32), 1)])
+                                        ((128, 128, 32), 1), ((48, 48, 12), 2), ((96, 96, 16), 2)])
 @pytest.mark.parametrize("precision", ["complex128", "mixed"])
 def test_batched_rhs_on_compile_time_kernels(sici, shape, nrhs, precision):
     """Batches on grids whose FFT lengths use the compile-time kernels."""

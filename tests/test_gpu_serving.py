@@ -108,6 +108,25 @@ def test_same_result_alone_and_in_the_mix(sici):
             assert i["status"] == "converged" and i["true_error"] <= r.tol
 
 
+def test_batch_of_different_wavelengths(sici):
+    """Same-grid requests with different wavelengths (so different tensors) run
+    as one batched solve, each right-hand side with its own tensor; each meets
+    its tolerance against the oracle and agrees with its solve alone."""
+    reqs = [_request((16, 16, 4), seed=50 + i, lam=480.0 + 60 * i, theta=7.0 * i) for i in range(3)]
+    with _server(sici=sici, workers=1) as srv:
+        alone = [srv.solve(r) for r in reqs]
+    with _server(sici=sici, workers=1) as srv:
+        blocker = srv.submit(_request((24, 24, 8), seed=59))
+        tickets = [srv.submit(r) for r in reqs]
+        srv.wait(blocker)
+        mixed = [srv.wait(t) for t in tickets]
+    assert [m.batch_requests for m in mixed] == [3, 3, 3]
+    assert mixed[0].batch_rhs == 6
+    for r, a, m in zip(reqs, alone, mixed):
+        assert rel(m.P, a.P) < 1e3 * r.tol
+        _check_against_oracle(sici, r, m, 1e3 * r.tol)
+
+
 def test_tensor_cache_and_eviction(sici):
     from dda_model.serving import DDAServer
 

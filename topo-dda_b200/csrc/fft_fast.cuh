@@ -8,7 +8,7 @@
 // with any thread count: each thread owns one batch column b and walks the
 // butterflies i0, i0 + istep, ... of that column.
 // Radix plan: 256 = 16*16, 128 = 16*8, 64 = 8*8, 32 = 8*4, 16 = 16, and
-// 8/4/2/3 for the rest (lengths 2^a 3^b).
+// 8/4/2/3 for the rest (lengths 2^a 3^b, e.g. 192 = 16*4*3, 96 = 8*4*3).
 #pragma once
 
 #include "fft_smem.cuh"
@@ -133,63 +133,73 @@ __device__ __forceinline__ C *fast_stages_from(C *a, C *b, int col, int i0, int 
     }
 }
 
-// In-place variant for blocks with at least nb * L / R threads at every stage
-// (one butterfly per thread, held in registers across the barrier).  In the
-// first stage, positions n >= nvalid are read as zero (zero-padded input), so
-// they need not be initialised.
-template <int L, int P, int SIGN, typename C>
+// In-place variant: every butterfly of a stage is loaded into registers,
+// transformed, and stored after a barrier.  Thread t owns butterflies
+// t, t + NTH, ... (at most K per stage, K = ceil(NBMAX * (L / R) / NTH) for a
+// batch of at most NBMAX columns).  In the first stage, positions n >= nvalid
+// are read as zero (zero-padded input), so they need not be initialised.
+template <int L, int P, int SIGN, int NBMAX, int NTH, typename C>
 __device__ __forceinline__ void ip_stage(C *buf, int nb, int pstr, int bstr, const C *__restrict__ tw, int twstep,
                                          int nvalid, int nkeep) {
     constexpr int R = fast_radix(L / P);
     constexpr int LR = L / R;
     constexpr int TS = L / (P * R);
     constexpr bool last = (P * R == L);
-    const int w = threadIdx.x;
-    C a[R];
-    int base = -1, jpos = 0;
-    if (w < nb * LR) {
-        const int b = w % nb, i = w / nb;
-        const int k = i % P;
-        const C *col = buf + b * bstr;
+    constexpr int K = (NBMAX * LR + NTH - 1) / NTH;
+    C a[K][R];
+    int base[K], jpos[K];
 #pragma unroll
-        for (int r = 0; r < R; ++r) {
-            const int n = i + r * LR;
-            if (P == 1 && n >= nvalid) a[r] = czero<C>();
-            else a[r] = col[n * pstr];
-        }
-        if (P > 1 && k != 0) {
-            const int j1 = k * TS * twstep;
+    for (int q = 0; q < K; ++q) {
+        const int w = threadIdx.x + q * NTH;
+        base[q] = -1;
+        jpos[q] = 0;
+        if (w < nb * LR) {
+            const int b = w % nb, i = w / nb;
+            const int k = i % P;
+            const C *col = buf + b * bstr;
 #pragma unroll
-            for (int r = 1; r < R; ++r) a[r] = a[r] * twiddle<SIGN>(tw, r * j1);
+            for (int r = 0; r < R; ++r) {
+                const int n = i + r * LR;
+                if (P == 1 && n >= nvalid) a[q][r] = czero<C>();
+                else a[q][r] = col[n * pstr];
+            }
+            if (P > 1 && k != 0) {
+                const int j1 = k * TS * twstep;
+#pragma unroll
+                for (int r = 1; r < R; ++r) a[q][r] = a[q][r] * twiddle<SIGN>(tw, r * j1);
+            }
+            dft_fast<R, SIGN>(a[q]);
+            jpos[q] = (i - k) * R + k;
+            base[q] = b * bstr + jpos[q] * pstr;
         }
-        dft_fast<R, SIGN>(a);
-        jpos = (i - k) * R + k;
-        base = b * bstr + jpos * pstr;
     }
     __syncthreads();
-    if (base >= 0) {
 #pragma unroll
-        for (int r = 0; r < R; ++r)
-            if (!last || jpos + r * P < nkeep) buf[base + r * P * pstr] = a[r];
+    for (int q = 0; q < K; ++q) {
+        if (base[q] >= 0) {
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+                if (!last || jpos[q] + r * P < nkeep) buf[base[q] + r * P * pstr] = a[q][r];
+        }
     }
     __syncthreads();
 }
 
-template <int L, int P, int SIGN, typename C>
+template <int L, int P, int SIGN, int NBMAX, int NTH, typename C>
 __device__ __forceinline__ void ip_stages_from(C *buf, int nb, int pstr, int bstr, const C *tw, int twstep,
                                                int nvalid, int nkeep) {
     if constexpr (P < L) {
-        ip_stage<L, P, SIGN>(buf, nb, pstr, bstr, tw, twstep, nvalid, nkeep);
-        ip_stages_from<L, P * fast_radix(L / P), SIGN>(buf, nb, pstr, bstr, tw, twstep, nvalid, nkeep);
+        ip_stage<L, P, SIGN, NBMAX, NTH>(buf, nb, pstr, bstr, tw, twstep, nvalid, nkeep);
+        ip_stages_from<L, P * fast_radix(L / P), SIGN, NBMAX, NTH>(buf, nb, pstr, bstr, tw, twstep, nvalid, nkeep);
     }
 }
 
-// nvalid: inputs at n >= nvalid are zero (never read); nkeep: only outputs
-// n < nkeep are written by the last stage.
-template <int L, int SIGN, typename C>
+// nb <= NBMAX columns, blockDim.x == NTH; nvalid: inputs at n >= nvalid are
+// zero (never read); nkeep: only outputs n < nkeep are written by the last stage.
+template <int L, int SIGN, int NBMAX, int NTH, typename C>
 __device__ __forceinline__ void fft_ip(C *buf, int nb, int pstr, int bstr, const C *tw, int Lmax, int nvalid,
                                        int nkeep = L) {
-    ip_stages_from<L, 1, SIGN>(buf, nb, pstr, bstr, tw, Lmax / L, nvalid, nkeep);
+    ip_stages_from<L, 1, SIGN, NBMAX, NTH>(buf, nb, pstr, bstr, tw, Lmax / L, nvalid, nkeep);
 }
 
 // largest number of butterflies any stage of a length-L transform needs per column

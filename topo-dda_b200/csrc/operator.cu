@@ -124,7 +124,8 @@ __global__ void __launch_bounds__(NT) k_fwd_zy(ConvGeom g, C *__restrict__ T, co
         A[y * g.pA + z] = czero<C>();
     }
     __syncthreads();
-    fft_smem<-1, MAXI>(A, g.Lz, g.ny, 1, g.pA, tw, g.Lmax);
+    for (int y0 = 0; y0 < g.ny; y0 += g.YC)
+        fft_smem<-1, MAXI>(A + y0 * g.pA, g.Lz, min(g.YC, g.ny - y0), 1, g.pA, tw, g.Lmax);
     C *Tc = T + ((size_t)(rhs * 3 + c) * g.nx + x) * (size_t)g.Ly * g.Lz;
     for (int kz0 = 0; kz0 < g.Lz; kz0 += g.CK) {
         for (int e = threadIdx.x; e < g.ny * g.CK; e += NT) {
@@ -150,9 +151,25 @@ __device__ __forceinline__ void fold(int k, int L, int &fk, int &sgn) {
     else { fk = L - k; sgn = -1; }
 }
 
+// w (the 3 components of one right-hand side, CKx apart) <- A w for the folded
+// symmetric tensor entry a[6] with the parity signs of its off-diagonal terms
+template <typename C>
+__device__ __forceinline__ void mul_sym3(const C *__restrict__ a, typename RealOf<C>::type sxy,
+                                         typename RealOf<C>::type sxz, typename RealOf<C>::type syz, C *w, int CKx) {
+    C axx = a[0], axy = sxy * a[1], axz = sxz * a[2];
+    C ayy = a[3], ayz = syz * a[4], azz = a[5];
+    C bx = w[0], by = w[CKx], bz = w[2 * CKx];
+    w[0] = axx * bx + axy * by + axz * bz;
+    w[CKx] = axy * bx + ayy * by + ayz * bz;
+    w[2 * CKx] = axz * bx + ayz * by + azz * bz;
+}
+
+// Pass 2: x transforms, tensor multiply, inverse x transforms for one ky and
+// a chunk of kz.  tab != nullptr: right-hand side r uses its own tensor tab[r]
+// (same grid, another wavelength or period); else every one uses ahat.
 template <typename C>
 __global__ void __launch_bounds__(NT) k_xconv(ConvGeom g, C *__restrict__ T, const C *__restrict__ ahat,
-                                              const C *__restrict__ tw, int nrhs,
+                                              const C *const *__restrict__ tab, const C *__restrict__ tw, int nrhs,
                                               const SolverState *__restrict__ st) {
     using R = typename RealOf<C>::type;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -184,10 +201,16 @@ __global__ void __launch_bounds__(NT) k_xconv(ConvGeom g, C *__restrict__ T, con
         int fkx, sx, fkz, sz;
         fold(kx, g.Lx, fkx, sx);
         fold(kz0 + kl, g.Lz, fkz, sz);
-        const C *a = ahat + (((size_t)fky * g.hx + fkx) * g.hz + fkz) * 6;
+        const size_t ti = (((size_t)fky * g.hx + fkx) * g.hz + fkz) * 6;
+        C *v = Cb + kx * pC + kl;
+        if (tab != nullptr) {
+            for (int r = 0; r < nrhs; ++r)
+                mul_sym3(tab[r] + ti, (R)(sx * sy), (R)(sx * sz), (R)(sy * sz), v + r * 3 * CKx, CKx);
+            continue;
+        }
+        const C *a = ahat + ti;
         C axx = a[0], axy = (R)(sx * sy) * a[1], axz = (R)(sx * sz) * a[2];
         C ayy = a[3], ayz = (R)(sy * sz) * a[4], azz = a[5];
-        C *v = Cb + kx * pC + kl;
         for (int r = 0; r < nrhs; ++r) {
             C *w = v + r * 3 * CKx;
             C bx = w[0], by = w[CKx], bz = w[2 * CKx];
@@ -212,8 +235,8 @@ constexpr int NT2 = 256;
 
 template <typename C, int L>
 __global__ void __launch_bounds__(NT2) k_xconv_fast(ConvGeom g, C *__restrict__ T, const C *__restrict__ ahat,
-                                                    const C *__restrict__ tw, int nrhs,
-                                                    const SolverState *__restrict__ st) {
+                                                    const C *const *__restrict__ tab, const C *__restrict__ tw,
+                                                    int nrhs, const SolverState *__restrict__ st) {
     using R = typename RealOf<C>::type;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     if (st != nullptr) {
@@ -241,10 +264,16 @@ __global__ void __launch_bounds__(NT2) k_xconv_fast(ConvGeom g, C *__restrict__ 
         int fkx, sx, fkz, sz;
         fold(kx, L, fkx, sx);
         fold(kz0 + kl, g.Lz, fkz, sz);
-        const C *a = ahat + (((size_t)fky * g.hx + fkx) * g.hz + fkz) * 6;
+        const size_t ti = (((size_t)fky * g.hx + fkx) * g.hz + fkz) * 6;
+        C *v = f + kx * nbat + kl;
+        if (tab != nullptr) {
+            for (int r = 0; r < nrhs; ++r)
+                mul_sym3(tab[r] + ti, (R)(sx * sy), (R)(sx * sz), (R)(sy * sz), v + r * 3 * CKx, CKx);
+            continue;
+        }
+        const C *a = ahat + ti;
         C axx = a[0], axy = (R)(sx * sy) * a[1], axz = (R)(sx * sz) * a[2];
         C ayy = a[3], ayz = (R)(sy * sz) * a[4], azz = a[5];
-        C *v = f + kx * nbat + kl;
         for (int r = 0; r < nrhs; ++r) {
             C *w = v + r * 3 * CKx;
             C bx = w[0], by = w[CKx], bz = w[2 * CKx];
@@ -263,19 +292,21 @@ __global__ void __launch_bounds__(NT2) k_xconv_fast(ConvGeom g, C *__restrict__ 
 }
 
 template <typename C>
-static bool launch_xconv_fast(const ConvGeom &g, C *T, const C *ahat, const C *tw, int nrhs,
+static bool launch_xconv_fast(const ConvGeom &g, C *T, const C *ahat, const C *const *tab, const C *tw, int nrhs,
                               const SolverState *st, cudaStream_t s) {
     dim3 grid(g.Ly, g.Lz / g.CKx2, 1);
     switch (g.Lx) {
-        case 256: k_xconv_fast<C, 256><<<grid, NT2, g.smem_x2, s>>>(g, T, ahat, tw, nrhs, st); return true;
-        case 128: k_xconv_fast<C, 128><<<grid, NT2, g.smem_x2, s>>>(g, T, ahat, tw, nrhs, st); return true;
-        case 64: k_xconv_fast<C, 64><<<grid, NT2, g.smem_x2, s>>>(g, T, ahat, tw, nrhs, st); return true;
-        case 32: k_xconv_fast<C, 32><<<grid, NT2, g.smem_x2, s>>>(g, T, ahat, tw, nrhs, st); return true;
+        case 256: k_xconv_fast<C, 256><<<grid, NT2, g.smem_x2, s>>>(g, T, ahat, tab, tw, nrhs, st); return true;
+        case 128: k_xconv_fast<C, 128><<<grid, NT2, g.smem_x2, s>>>(g, T, ahat, tab, tw, nrhs, st); return true;
+        case 64: k_xconv_fast<C, 64><<<grid, NT2, g.smem_x2, s>>>(g, T, ahat, tab, tw, nrhs, st); return true;
+        case 32: k_xconv_fast<C, 32><<<grid, NT2, g.smem_x2, s>>>(g, T, ahat, tab, tw, nrhs, st); return true;
+        case 192: k_xconv_fast<C, 192><<<grid, NT2, g.smem_x2, s>>>(g, T, ahat, tab, tw, nrhs, st); return true;
+        case 96: k_xconv_fast<C, 96><<<grid, NT2, g.smem_x2, s>>>(g, T, ahat, tab, tw, nrhs, st); return true;
         default: return false;
     }
 }
 
-static bool fast_x_length(int L) { return L == 256 || L == 128 || L == 64 || L == 32; }
+static bool fast_x_length(int L) { return L == 256 || L == 192 || L == 128 || L == 96 || L == 64 || L == 32; }
 
 // Passes 1 and 3 for complex64 with compile-time (Lz, Ly): the whole padded
 // (x, component) slab [Ly][Lz + 1] sits in shared memory and 1024 threads
@@ -299,8 +330,9 @@ __global__ void __launch_bounds__(NT3, 1) k_fwd_zy_fast(ConvGeom g, C *__restric
         S[y * pS + z] = pro.load(rhs, c, cell0 + e);
     }
     __syncthreads();
-    fft_ip<LZ, -1>(S, g.ny, 1, pS, tw, g.Lmax, g.nz);
-    fft_ip<LY, -1>(S, LZ, pS, 1, tw, g.Lmax, g.ny);
+    // ny <= (LY + 1) / 2 columns of z, LZ columns of y
+    fft_ip<LZ, -1, (LY + 1) / 2, NT3>(S, g.ny, 1, pS, tw, g.Lmax, g.nz);
+    fft_ip<LY, -1, LZ, NT3>(S, LZ, pS, 1, tw, g.Lmax, g.ny);
     C *Tc = T + ((size_t)(rhs * 3 + c) * g.nx + x) * (size_t)(LY * LZ);
     for (int e = threadIdx.x; e < LY * LZ; e += NT3) Tc[e] = S[(e / LZ) * pS + (e % LZ)];
 }
@@ -316,8 +348,8 @@ __global__ void __launch_bounds__(NT3, 1) k_inv_yz_fast(ConvGeom g, const C *__r
     const C *Tc = T + ((size_t)(rhs * 3 + c) * g.nx + x) * (size_t)(LY * LZ);
     for (int e = threadIdx.x; e < LY * LZ; e += NT3) S[(e / LZ) * pS + (e % LZ)] = Tc[e];
     __syncthreads();
-    fft_ip<LY, +1>(S, LZ, pS, 1, tw, g.Lmax, LY, g.ny);
-    fft_ip<LZ, +1>(S, g.ny, 1, pS, tw, g.Lmax, LZ, g.nz);
+    fft_ip<LY, +1, LZ, NT3>(S, LZ, pS, 1, tw, g.Lmax, LY, g.ny);
+    fft_ip<LZ, +1, (LY + 1) / 2, NT3>(S, g.ny, 1, pS, tw, g.Lmax, LZ, g.nz);
     const int nyz = g.ny * g.nz;
     const long long cell0 = (long long)x * nyz;
     double2 acc[Epi::NQ > 0 ? Epi::NQ : 1];
@@ -334,7 +366,7 @@ __global__ void __launch_bounds__(NT3, 1) k_inv_yz_fast(ConvGeom g, const C *__r
 }
 
 // (Lz, Ly) pairs with a compile-time slab kernel
-#define TDDA_YZ_PAIRS(X) X(64, 256) X(32, 128) X(16, 64) X(16, 32)
+#define TDDA_YZ_PAIRS(X) X(64, 256) X(32, 128) X(16, 64) X(16, 32) X(24, 96) X(32, 192) X(48, 192) X(32, 256)
 
 static bool fast_yz_pair(int Lz, int Ly) {
 #define TDDA_PAIR_TEST(a, b) if (Lz == a && Ly == b) return true;
@@ -397,7 +429,8 @@ __global__ void __launch_bounds__(NT) k_inv_yz(ConvGeom g, const C *__restrict__
         }
         __syncthreads();
     }
-    fft_smem<+1, MAXI>(A, g.Lz, g.ny, 1, g.pA, tw, g.Lmax);
+    for (int y0 = 0; y0 < g.ny; y0 += g.YC)
+        fft_smem<+1, MAXI>(A + y0 * g.pA, g.Lz, min(g.YC, g.ny - y0), 1, g.pA, tw, g.Lmax);
     const int nyz = g.ny * g.nz;
     const long long cell0 = (long long)x * nyz;
     double2 acc[Epi::NQ > 0 ? Epi::NQ : 1];
@@ -722,6 +755,8 @@ template <typename C> static void set_smem_attrs(int yz, int x) {
     cudaFuncSetAttribute(k_xconv_fast<C, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, x);
     cudaFuncSetAttribute(k_xconv_fast<C, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, x);
     cudaFuncSetAttribute(k_xconv_fast<C, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, x);
+    cudaFuncSetAttribute(k_xconv_fast<C, 192>, cudaFuncAttributeMaxDynamicSharedMemorySize, x);
+    cudaFuncSetAttribute(k_xconv_fast<C, 96>, cudaFuncAttributeMaxDynamicSharedMemorySize, x);
     if constexpr (std::is_same<C, float2>::value) {
         // dynamic + static shared memory must stay within the 227 KB opt-in limit;
         // the epilogue kernels carry ~1 KB of static reduction scratch
@@ -750,7 +785,10 @@ static bool plan_geom(int nx, int ny, int nz, int nrhs, int esize, ConvGeom &g, 
     g.tcomp = (long long)nx * g.Ly * g.Lz;
     g.nrhs = nrhs;
     g.pA = (g.Lz % 2 == 0) ? g.Lz + 1 : g.Lz;
-    if (fft_max_items(g.Lz, ny, NT) > MAXI) { why = "ny too large for the z transform"; return false; }
+    // z transforms of the slab in chunks of YC columns (as many as fit the block)
+    g.YC = ny;
+    while (g.YC > 1 && fft_max_items(g.Lz, g.YC, NT) > MAXI) g.YC = (g.YC + 1) / 2;
+    if (fft_max_items(g.Lz, g.YC, NT) > MAXI) { why = "Lz too large for the z transform"; return false; }
     g.CK = 0;
     for (int ck = g.Lz; ck >= 1; --ck) {
         if (g.Lz % ck) continue;
@@ -779,10 +817,7 @@ static bool plan_geom(int nx, int ny, int nz, int nrhs, int esize, ConvGeom &g, 
     g.smem_x = g.Lx * g.pC * esize;
     // compile-time slab kernels for passes 1 and 3 (complex64 only)
     g.smem_yz2 = (int)((long long)g.Ly * (g.Lz + 1) * esize);
-    g.fast_yz = (esize == 8 && fast_yz_pair(g.Lz, g.Ly) && g.smem_yz2 <= kSmemFast &&
-                 ny * fast_max_items(g.Lz) <= NT3 && g.Lz * fast_max_items(g.Ly) <= NT3)
-                    ? 1
-                    : 0;
+    g.fast_yz = (esize == 8 && fast_yz_pair(g.Lz, g.Ly) && g.smem_yz2 <= kSmemFast) ? 1 : 0;
     // compile-time-length pass 2: two ping-pong buffers, at most ~100 KB so
     // that two CTAs share an SM; runs of >= 64 bytes along kz
     g.fast_x = fast_x_length(g.Lx) ? 1 : 0;
@@ -858,8 +893,8 @@ static tdda_status run_conv(ConvOperator<C> &op, const ConvGeom &g, int nrhs, co
         k_fwd_zy<C, Pro><<<g13, NT, g.smem_yz, s>>>(g, op.T, op.tw, pro);
     dim3 g2(g.Ly, g.Lz / g.CKx, 1);
     count_launches(1);
-    if (!(g.fast_x && launch_xconv_fast<C>(g, op.T, op.ahat, op.tw, nrhs, st, s)))
-        k_xconv<C><<<g2, NT, g.smem_x, s>>>(g, op.T, op.ahat, op.tw, nrhs, st);
+    if (!(g.fast_x && launch_xconv_fast<C>(g, op.T, op.ahat, op.ahat_rhs, op.tw, nrhs, st, s)))
+        k_xconv<C><<<g2, NT, g.smem_x, s>>>(g, op.T, op.ahat, op.ahat_rhs, op.tw, nrhs, st);
     count_launches(1);
     if (!(g.fast_yz && launch_inv_fast<C, Epi>(g, g13, op.T, op.tw, epi, s)))
         k_inv_yz<C, Epi><<<g13, NT, g.smem_yz, s>>>(g, op.T, op.tw, epi);
@@ -1091,8 +1126,8 @@ tdda_status profile_apply(ConvOperator<C> &op, const C *x, C *y, const C *al, in
     });
     ms_pass[1] = timed([&] {
         count_launches(1);
-        if (!(g.fast_x && launch_xconv_fast<C>(g, op.T, op.ahat, op.tw, nrhs, nullptr, s)))
-            k_xconv<C><<<g2, NT, g.smem_x, s>>>(g, op.T, op.ahat, op.tw, nrhs, nullptr);
+        if (!(g.fast_x && launch_xconv_fast<C>(g, op.T, op.ahat, op.ahat_rhs, op.tw, nrhs, nullptr, s)))
+            k_xconv<C><<<g2, NT, g.smem_x, s>>>(g, op.T, op.ahat, op.ahat_rhs, op.tw, nrhs, nullptr);
     });
     ms_pass[2] = timed([&] {
         count_launches(1);

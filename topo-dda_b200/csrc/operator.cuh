@@ -29,6 +29,7 @@ struct SolverState {
 template <typename C> struct ConvOperator {
     ConvGeom g{};
     C *ahat = nullptr;     // folded spectral tensor [hy][hx][hz][6], scaled by 1/(Lx Ly Lz)
+    const C *const *ahat_rhs = nullptr;  // device table of one tensor per right-hand side, or nullptr
     C *tw = nullptr;       // twiddles exp(-2 pi i j / Lmax), j < Lmax
     C *T = nullptr;        // spectral intermediate, nrhs_cap * 3 * tcomp
     int nrhs_cap = 0;

@@ -13,9 +13,12 @@
 //     solve workspace per grid shape it has served (sized for max_rhs);
 //   * one FIFO queue; an idle worker admits the first request whose device
 //     memory (tensor if not resident + its workspace if not yet allocated) fits
-//     the budget, evicting idle tensors (LRU) and its own idle workspaces of
-//     other shapes when short, then merges every queued request with the same
-//     tensor key (and precision, tolerance, iteration limit) into the batch;
+//     the budget, evicting idle tensors (LRU) and idle workspaces of other
+//     shapes when short, then merges queued requests of the same grid (and
+//     precision, tolerance, iteration limit) into the batch, up to the most
+//     right-hand sides the operator takes for that grid.  Each right-hand side
+//     keeps its own tensor (its wavelength and period); requests with equal
+//     tensor keys share one;
 //   * a tensor is built once per key on the admitting worker's stream; other
 //     workers needing it wait until it is ready and then share it read-only.
 #include <algorithm>
@@ -171,6 +174,9 @@ struct Workspace {
     double *d_part = nullptr, *h_part = nullptr;
     double *d_rho = nullptr, *h_rho = nullptr;
     double2 *d_out = nullptr, *h_out = nullptr;  // P then E, [cap][3 nbox] each
+    const double2 **h_tab64 = nullptr, **d_tab64 = nullptr;  // tensor of each right-hand side
+    const float2 **h_tab32 = nullptr, **d_tab32 = nullptr;
+    bool want64 = false;  // complex128 part reserved, allocated at first use
     size_t bytes = 0;
 
     static size_t bytes_for(int nx, int ny, int nz, int cap) {
@@ -221,6 +227,10 @@ struct Workspace {
         TDDA_CUDA_TRY(cudaMallocHost(&h_rho, sizeof(double) * d));
         TDDA_CUDA_TRY(cudaMalloc(&d_out, sizeof(double2) * 2 * v));
         TDDA_CUDA_TRY(cudaMallocHost(&h_out, sizeof(double2) * 2 * v));
+        TDDA_CUDA_TRY(cudaMalloc(&d_tab64, sizeof(void *) * cap));
+        TDDA_CUDA_TRY(cudaMalloc(&d_tab32, sizeof(void *) * cap));
+        TDDA_CUDA_TRY(cudaMallocHost(&h_tab64, sizeof(void *) * cap));
+        TDDA_CUDA_TRY(cudaMallocHost(&h_tab32, sizeof(void *) * cap));
         bytes = bytes_for(nx, ny, nz, cap);
         return TDDA_OK;
     }
@@ -246,9 +256,9 @@ struct Workspace {
         kv32.release();
         kv64.release();
         void *dev[] = {B, X, Rm, al64, sc64, diel, alS64, R64, D64, al32, sc32, alS32, R32, D32, st_res, d_part,
-                       d_rho, d_out};
+                       d_rho, d_out, (void *)d_tab64, (void *)d_tab32};
         for (void *p : dev) cudaFree(p);
-        void *host[] = {st_res_host, h_part, h_rho, h_out};
+        void *host[] = {st_res_host, h_part, h_rho, h_out, (void *)h_tab64, (void *)h_tab32};
         for (void *p : host) cudaFreeHost(p);
     }
 };
@@ -263,9 +273,13 @@ struct Job {
     std::string error;
     int rhs_cap = 1;  // most right-hand sides a batch of this grid may hold
     bool done = false;
+    std::shared_ptr<Tensor> tensor;  // held from admission to the end of its batch
+    bool hit = false;
 };
 
 using Shape = std::tuple<int, int, int>;
+
+Shape shape_of(const tdda_request &r) { return Shape{r.num_x, r.num_y, r.num_z}; }
 
 struct Worker {
     int id = 0;
@@ -291,44 +305,52 @@ struct tdda_server {
     std::list<std::shared_ptr<Tensor>> cache;  // least recently used first
     std::vector<std::unique_ptr<Worker>> workers;
     long long next_ticket = 1;
-    unsigned long long tick = 0;
     size_t in_use = 0;
     int inflight = 0;
     bool stop = false;
     tdda_server_stats stats{};
+
+    using FreeList = std::vector<std::unique_ptr<Workspace>>;
+    using EvictList = std::vector<std::shared_ptr<Tensor>>;
 
     std::shared_ptr<Tensor> find(const TensorKey &k) {
         for (auto &t : cache)
             if (t->key == k) return t;
         return nullptr;
     }
+    long long need_of(Worker *w, const Job &j, bool with_ws);
+    bool make_room(Worker *w, size_t need, const Shape &keep, FreeList &to_free, EvictList &evicted);
+    void take(Worker *w, Job &j, bool with_ws, size_t need);
     void run(Worker *w);
-    bool admit(Worker *w, const std::shared_ptr<Job> &j, std::shared_ptr<Tensor> &t, bool &hit,
-               std::vector<std::unique_ptr<Workspace>> &to_free, std::vector<std::shared_ptr<Tensor>> &evicted);
-    void run_batch(Worker *w, std::vector<std::shared_ptr<Job>> &batch, std::shared_ptr<Tensor> t, bool hit);
+    void run_batch(Worker *w, std::vector<std::shared_ptr<Job>> &batch);
 };
 
-// Under the lock: reserve device memory for job j on worker w.  Returns false
-// when it cannot run now (tensor being built elsewhere, or memory short with
-// nothing idle left to evict).
-bool tdda_server::admit(Worker *w, const std::shared_ptr<Job> &j, std::shared_ptr<Tensor> &t, bool &hit,
-                        std::vector<std::unique_ptr<Workspace>> &to_free,
-                        std::vector<std::shared_ptr<Tensor>> &evicted) {
-    const tdda_request &r = j->req;
-    const Shape shape{r.num_x, r.num_y, r.num_z};
-    t = find(j->key);
-    if (t && (!t->ready || t->failed)) return false;
-    size_t need = 0;
-    auto it = w->ws.find(shape);
-    const bool need_ws = (it == w->ws.end());
-    if (need_ws) need += Workspace::bytes_for(r.num_x, r.num_y, r.num_z, cfg.max_rhs);
-    if (r.precision == TDDA_PREC_C128 && (need_ws || !it->second->has64))
-        need += Workspace::bytes64_for(r.num_x, r.num_y, r.num_z, cfg.max_rhs);
-    if (!t) need += tensor_bytes(r.num_x, r.num_y, r.num_z);
+// Under the lock: device bytes job j still needs on worker w -- its tensor if
+// not resident, and (with_ws) the worker's workspace for its grid if missing
+// or without the complex128 part a complex128 request needs.  -1: its tensor
+// is being built by another worker right now.
+long long tdda_server::need_of(Worker *w, const Job &j, bool with_ws) {
+    const tdda_request &r = j.req;
+    auto t = find(j.key);
+    if (t && (!t->ready || t->failed)) return -1;
+    size_t need = t ? 0 : tensor_bytes(r.num_x, r.num_y, r.num_z);
+    if (with_ws) {
+        auto it = w->ws.find(shape_of(r));
+        const bool missing = it == w->ws.end();
+        if (missing) need += Workspace::bytes_for(r.num_x, r.num_y, r.num_z, cfg.max_rhs);
+        if (r.precision == TDDA_PREC_C128 && (missing || (!it->second->has64 && !it->second->want64)))
+            need += Workspace::bytes64_for(r.num_x, r.num_y, r.num_z, cfg.max_rhs);
+    }
+    return (long long)need;
+}
+
+// Under the lock: evict until `need` more bytes fit the budget -- idle
+// tensors least recently used first, then this worker's workspaces of other
+// grids, then, with no batch in flight, other workers' workspaces.
+bool tdda_server::make_room(Worker *w, size_t need, const Shape &keep, FreeList &to_free, EvictList &evicted) {
     const size_t budget = (size_t)cfg.hbm_budget_bytes;
-    // evict idle tensors, least recently used first
     for (auto c = cache.begin(); in_use + need > budget && c != cache.end();) {
-        if ((*c)->users == 0 && (*c)->ready && *c != t) {
+        if ((*c)->users == 0 && (*c)->ready) {
             in_use -= (*c)->bytes;
             evicted.push_back(*c);
             c = cache.erase(c);
@@ -337,9 +359,8 @@ bool tdda_server::admit(Worker *w, const std::shared_ptr<Job> &j, std::shared_pt
             ++c;
         }
     }
-    // then this worker's own (idle) workspaces of other shapes
     for (auto c = w->ws.begin(); in_use + need > budget && c != w->ws.end();) {
-        if (c->first != shape) {
+        if (c->first != keep) {
             in_use -= c->second->bytes;
             to_free.push_back(std::move(c->second));
             c = w->ws.erase(c);
@@ -347,7 +368,6 @@ bool tdda_server::admit(Worker *w, const std::shared_ptr<Job> &j, std::shared_pt
             ++c;
         }
     }
-    // with no batch in flight every workspace is idle: take other workers' too
     for (auto &ow : workers) {
         if (in_use + need <= budget || inflight > 0) break;
         if (ow.get() == w) continue;
@@ -357,30 +377,41 @@ bool tdda_server::admit(Worker *w, const std::shared_ptr<Job> &j, std::shared_pt
             c = ow->ws.erase(c);
         }
     }
-    if (in_use + need > budget) return false;
+    return in_use + need <= budget;
+}
+
+// Under the lock, after need_of/make_room: take job j's reservation of `need` bytes.
+void tdda_server::take(Worker *w, Job &j, bool with_ws, size_t need) {
+    const tdda_request &r = j.req;
     in_use += need;
     stats.peak_bytes = std::max<int64_t>(stats.peak_bytes, (int64_t)in_use);
+    auto t = find(j.key);
     if (t) {
-        hit = true;
+        j.hit = true;
         t->users++;
         stats.cache_hits++;
     } else {
-        hit = false;
+        j.hit = false;
         t = std::make_shared<Tensor>();
-        t->key = j->key;
+        t->key = j.key;
         t->bytes = tensor_bytes(r.num_x, r.num_y, r.num_z);
         t->users = 1;
         cache.push_back(t);
         stats.cache_misses++;
     }
-    if (need_ws) {
-        // reserve now, allocate outside the lock: an empty placeholder marks it
-        w->ws[shape] = std::unique_ptr<Workspace>(new Workspace());
-        w->ws[shape]->bytes = Workspace::bytes_for(r.num_x, r.num_y, r.num_z, cfg.max_rhs);
+    j.tensor = t;
+    if (with_ws) {
+        auto &slot = w->ws[shape_of(r)];
+        if (!slot) {
+            // reserved now, allocated by the worker outside the lock
+            slot.reset(new Workspace());
+            slot->bytes = Workspace::bytes_for(r.num_x, r.num_y, r.num_z, cfg.max_rhs);
+        }
+        if (r.precision == TDDA_PREC_C128 && !slot->has64 && !slot->want64) {
+            slot->want64 = true;
+            slot->bytes += Workspace::bytes64_for(r.num_x, r.num_y, r.num_z, cfg.max_rhs);
+        }
     }
-    if (r.precision == TDDA_PREC_C128 && !w->ws[shape]->has64)
-        w->ws[shape]->bytes += Workspace::bytes64_for(r.num_x, r.num_y, r.num_z, cfg.max_rhs);
-    return true;
 }
 
 void tdda_server::run(Worker *w) {
@@ -388,27 +419,31 @@ void tdda_server::run(Worker *w) {
     std::unique_lock<std::mutex> lk(mu);
     for (;;) {
         if (stop && queue.empty()) return;
-        std::shared_ptr<Tensor> t;
-        bool hit = false;
-        std::vector<std::unique_ptr<Workspace>> to_free;
-        std::vector<std::shared_ptr<Tensor>> evicted;
+        FreeList to_free;
+        EvictList evicted;
         std::vector<std::shared_ptr<Job>> batch;
         for (auto q = queue.begin(); q != queue.end(); ++q) {
-            if (admit(w, *q, t, hit, to_free, evicted)) {
+            const long long need = need_of(w, **q, true);
+            if (need >= 0 && make_room(w, (size_t)need, shape_of((*q)->req), to_free, evicted)) {
+                take(w, **q, true, (size_t)need);
                 batch.push_back(*q);
                 queue.erase(q);
                 break;
             }
             if (q == queue.begin()) stats.admission_waits++;
         }
+        auto release = [&]() {
+            to_free.clear();
+            for (auto &e : evicted) {
+                cudaFreeAsync(e->ahat64, w->stream);
+                cudaFreeAsync(e->ahat32, w->stream);
+            }
+            evicted.clear();
+        };
         if (batch.empty()) {
             if (!to_free.empty() || !evicted.empty()) {
                 lk.unlock();
-                to_free.clear();
-                for (auto &e : evicted) {
-                    cudaFreeAsync(e->ahat64, w->stream);
-                    cudaFreeAsync(e->ahat32, w->stream);
-                }
+                release();
                 cudaStreamSynchronize(w->stream);
                 lk.lock();
                 continue;
@@ -416,20 +451,35 @@ void tdda_server::run(Worker *w) {
             cv_work.wait(lk);
             continue;
         }
-        // continuous batching: queued requests with the same tensor join
+        // continuous batching: queued requests of the same grid join as further
+        // right-hand sides, each with its own tensor (shared when the keys match)
         const tdda_request &r0 = batch[0]->req;
+        const Shape sh = shape_of(r0);
         int rhs = r0.npol;
+        // a tensor that this batch itself is about to build is shared, not waited for
+        auto built_here = [&](const Job &j) {
+            auto t = find(j.key);
+            if (!t || t->ready) return false;
+            for (auto &b : batch)
+                if (b->tensor == t) return true;
+            return false;
+        };
         for (auto q = queue.begin(); q != queue.end();) {
             const tdda_request &r = (*q)->req;
-            if ((*q)->key == batch[0]->key && r.precision == r0.precision && r.tol == r0.tol &&
-                r.max_iter == r0.max_iter && rhs + r.npol <= batch[0]->rhs_cap) {
-                rhs += r.npol;
-                batch.push_back(*q);
-                q = queue.erase(q);
-                stats.merged_requests++;
-            } else {
-                ++q;
+            bool joined = false;
+            if (shape_of(r) == sh && r.precision == r0.precision && r.tol == r0.tol && r.max_iter == r0.max_iter &&
+                rhs + r.npol <= batch[0]->rhs_cap) {
+                const long long need = built_here(**q) ? 0 : need_of(w, **q, false);
+                if (need >= 0 && make_room(w, (size_t)need, sh, to_free, evicted)) {
+                    take(w, **q, false, (size_t)need);
+                    rhs += r.npol;
+                    batch.push_back(*q);
+                    q = queue.erase(q);
+                    stats.merged_requests++;
+                    joined = true;
+                }
             }
+            if (!joined) ++q;
         }
         const auto now = Clock::now();
         for (auto &j : batch) j->t_admit = now;
@@ -437,41 +487,33 @@ void tdda_server::run(Worker *w) {
         inflight++;
         stats.max_concurrent = std::max(stats.max_concurrent, inflight);
         lk.unlock();
-        to_free.clear();
-        for (auto &e : evicted) {
-            cudaFreeAsync(e->ahat64, w->stream);
-            cudaFreeAsync(e->ahat32, w->stream);
-        }
-        run_batch(w, batch, t, hit);
+        release();
+        run_batch(w, batch);
         lk.lock();
         inflight--;
-        t->users--;
-        t->last_use = ++tick;
-        // most recently used to the back
-        for (auto c = cache.begin(); c != cache.end(); ++c)
-            if (*c == t) {
-                cache.erase(c);
-                break;
-            }
-        if (t->failed) {
-            in_use -= t->bytes;
-        } else {
-            cache.push_back(t);
-        }
-        stats.cached_tensors = (int64_t)cache.size();
-        stats.bytes_in_use = (int64_t)in_use;
         for (auto &j : batch) {
+            std::shared_ptr<Tensor> t = j->tensor;
+            j->tensor.reset();
+            t->users--;
+            for (auto c = cache.begin(); c != cache.end(); ++c)
+                if (*c == t) {
+                    cache.erase(c);
+                    if (t->failed) in_use -= t->bytes;
+                    else cache.push_back(t);  // most recently used last
+                    break;
+                }
             j->done = true;
             stats.completed++;
             if (j->res.status != TDDA_OK) stats.failed++;
         }
+        stats.cached_tensors = (int64_t)cache.size();
+        stats.bytes_in_use = (int64_t)in_use;
         cv_done.notify_all();
         cv_work.notify_all();
     }
 }
 
-void tdda_server::run_batch(Worker *w, std::vector<std::shared_ptr<Job>> &batch, std::shared_ptr<Tensor> t,
-                            bool hit) {
+void tdda_server::run_batch(Worker *w, std::vector<std::shared_ptr<Job>> &batch) {
     const tdda_request &r0 = batch[0]->req;
     const int nx = r0.num_x, ny = r0.num_y, nz = r0.num_z;
     const long long nbox = (long long)nx * ny * nz;
@@ -486,7 +528,7 @@ void tdda_server::run_batch(Worker *w, std::vector<std::shared_ptr<Job>> &batch,
     Workspace *ws = nullptr;
     {
         std::lock_guard<std::mutex> g(mu);
-        ws = w->ws[Shape{nx, ny, nz}].get();
+        ws = w->ws[shape_of(r0)].get();
     }
     tdda_status st = TDDA_OK;
     if (ws->cap == 0) {
@@ -497,13 +539,15 @@ void tdda_server::run_batch(Worker *w, std::vector<std::shared_ptr<Job>> &batch,
             const std::string msg = get_error();
             std::lock_guard<std::mutex> g(mu);
             in_use -= ws->bytes;
-            w->ws.erase(Shape{nx, ny, nz});
-            if (!hit) t->failed = true;
+            w->ws.erase(shape_of(r0));
+            for (auto &j : batch)
+                if (!j->hit) j->tensor->failed = true;
             fail(st, msg);
             return;
         }
     }
-    if (r0.precision == TDDA_PREC_C128 && !ws->has64) {
+    const bool c128 = r0.precision == TDDA_PREC_C128;
+    if (c128 && !ws->has64) {
         const size_t reserved = ws->bytes;
         st = ws->init64();
         ws->bytes = reserved;
@@ -512,50 +556,59 @@ void tdda_server::run_batch(Worker *w, std::vector<std::shared_ptr<Job>> &batch,
             return;
         }
     }
-    // tensor
-    const auto tb0 = Clock::now();
-    double build_ms = 0.0;
-    if (!hit) {
-        const ConvGeom &g = ws->op64.g;
-        const size_t nfold = (size_t)g.hx * g.hy * g.hz * 6;
-        bool ok = cudaMallocAsync(&t->ahat64, sizeof(double2) * nfold, s) == cudaSuccess &&
-                  cudaMallocAsync(&t->ahat32, sizeof(float2) * nfold, s) == cudaSuccess;
+    // tensors of the requests that missed the cache, one after another on this stream
+    const ConvGeom &g = ws->op64.g;
+    const size_t nfold = (size_t)g.hx * g.hy * g.hz * 6;
+    std::vector<double> build_ms(batch.size(), 0.0);
+    for (size_t jj = 0; jj < batch.size(); ++jj) {
+        Job &j = *batch[jj];
+        if (j.hit) continue;
+        Tensor &t = *j.tensor;
+        const auto tb0 = Clock::now();
+        const tdda_request &r = j.req;
+        bool ok = cudaMallocAsync(&t.ahat64, sizeof(double2) * nfold, s) == cudaSuccess &&
+                  cudaMallocAsync(&t.ahat32, sizeof(float2) * nfold, s) == cudaSuccess;
         LatticeParams L{};
         L.nx = nx; L.ny = ny; L.nz = nz;
         L.Lx = g.Lx; L.Ly = g.Ly; L.Lz = g.Lz;
-        L.d = r0.d; L.K = 2.0 * M_PI / (r0.lam / r0.nback); L.Kf = M_PI / r0.d;
-        L.Lm = r0.Lm * r0.d; L.Ln = r0.Ln * r0.d;
-        L.MAXm = r0.MAXm; L.MAXn = r0.MAXn; L.method = r0.method; L.gamma = 0.01; L.delta = delta;
+        L.d = r.d; L.K = 2.0 * M_PI / (r.lam / r.nback); L.Kf = M_PI / r.d;
+        L.Lm = r.Lm * r.d; L.Ln = r.Ln * r.d;
+        L.MAXm = r.MAXm; L.MAXn = r.MAXn; L.method = r.method; L.gamma = 0.01; L.delta = delta;
         if (ok) {
             w->scratch.sc = d_sici;
             w->scratch.ntab = ntab;
-            st = build_tensor_async(L, w->scratch, t->ahat64, t->ahat32, s, w->a0_host, nullptr, nullptr);
-            ok = st == TDDA_OK && cudaStreamSynchronize(s) == cudaSuccess;
+            ok = build_tensor_async(L, w->scratch, t.ahat64, t.ahat32, s, w->a0_host, nullptr, nullptr) == TDDA_OK &&
+                 cudaStreamSynchronize(s) == cudaSuccess;
         }
         std::lock_guard<std::mutex> g2(mu);
         if (!ok) {
-            t->failed = true;
-            cudaFreeAsync(t->ahat64, s);
-            cudaFreeAsync(t->ahat32, s);
-            t->ahat64 = nullptr;
-            t->ahat32 = nullptr;
+            // every tensor of this batch not built yet is abandoned with it
+            for (auto &o : batch)
+                if (!o->tensor->ready) o->tensor->failed = true;
+            cudaFreeAsync(t.ahat64, s);
+            cudaFreeAsync(t.ahat32, s);
+            t.ahat64 = nullptr;
+            t.ahat32 = nullptr;
             fail(TDDA_ERR_CUDA, std::string("tensor build failed: ") + get_error());
             cv_work.notify_all();
             return;
         }
         const double2 *a = w->a0_host;
-        t->a0 = make_double2((a[0].x + a[3].x + a[5].x) / 3.0, (a[0].y + a[3].y + a[5].y) / 3.0);
-        t->ready = true;
+        t.a0 = make_double2((a[0].x + a[3].x + a[5].x) / 3.0, (a[0].y + a[3].y + a[5].y) / 3.0);
+        t.ready = true;
         cv_work.notify_all();  // workers waiting for this tensor
-        build_ms = ms_between(tb0, Clock::now());
+        build_ms[jj] = ms_between(tb0, Clock::now());
     }
     const auto ts0 = Clock::now();
-    // per right-hand side parameters and densities
+    // per right-hand side parameters, densities and tensors
     SetupArgs sa{};
     sa.nx = nx; sa.ny = ny; sa.nz = nz;
     int k = 0;
+    bool shared = true;
     for (size_t jj = 0; jj < batch.size(); ++jj) {
         const tdda_request &r = batch[jj]->req;
+        const Tensor &t = *batch[jj]->tensor;
+        shared &= (batch[jj]->tensor == batch[0]->tensor);
         std::memcpy(ws->h_rho + jj * (size_t)nbox, batch[jj]->rho.data(), sizeof(double) * nbox);
         const double K = 2.0 * M_PI / (r.lam / r.nback);
         double2 m[2];
@@ -570,24 +623,31 @@ void tdda_server::run_batch(Worker *w, std::vector<std::shared_ptr<Job>> &batch,
             p.A.lam = r.lam; p.A.K = K; p.A.d = r.d; p.A.m0 = m[0]; p.A.m1 = m[1];
             p.A.S = 0.0;
             for (int c = 0; c < 3; ++c) p.A.S += std::pow(r.n_E0[q][c] * r.n_K[c], 2);
-            p.a0 = t->a0;
+            p.a0 = t.a0;
             p.kd = K * r.d;
             for (int c = 0; c < 3; ++c) {
                 p.nK[c] = r.n_K[c];
                 p.e[c] = r.E0 * r.n_E0[q][c];
             }
             p.job = (int)jj;
+            ws->h_tab64[k] = t.ahat64;
+            ws->h_tab32[k] = t.ahat32;
         }
     }
     const int nrhs = k;
     sa.nrhs = nrhs;
-    ws->op64.ahat = t->ahat64;
-    ws->op32.ahat = t->ahat32;
-    const bool c128 = r0.precision == TDDA_PREC_C128;
+    ws->op64.ahat = batch[0]->tensor->ahat64;
+    ws->op32.ahat = batch[0]->tensor->ahat32;
+    ws->op64.ahat_rhs = shared ? nullptr : ws->d_tab64;
+    ws->op32.ahat_rhs = shared ? nullptr : ws->d_tab32;
     std::vector<tdda_solve_info> info(nrhs);
     st = TDDA_OK;
     if (cudaMemcpyAsync(ws->d_rho, ws->h_rho, sizeof(double) * nbox * batch.size(), cudaMemcpyHostToDevice, s) !=
-        cudaSuccess)
+            cudaSuccess ||
+        (!shared && (cudaMemcpyAsync(ws->d_tab64, ws->h_tab64, sizeof(void *) * nrhs, cudaMemcpyHostToDevice, s) !=
+                         cudaSuccess ||
+                     cudaMemcpyAsync(ws->d_tab32, ws->h_tab32, sizeof(void *) * nrhs, cudaMemcpyHostToDevice, s) !=
+                         cudaSuccess)))
         st = TDDA_ERR_CUDA;
     if (st == TDDA_OK) {
         count_launches(1);
@@ -633,23 +693,24 @@ void tdda_server::run_batch(Worker *w, std::vector<std::shared_ptr<Job>> &batch,
     const size_t v = 3 * (size_t)nbox * nrhs;
     const auto done = Clock::now();
     k = 0;
-    for (auto &j : batch) {
-        const tdda_request &r = j->req;
+    for (size_t jj = 0; jj < batch.size(); ++jj) {
+        Job &j = *batch[jj];
+        const tdda_request &r = j.req;
         const size_t n3 = 3 * (size_t)nbox;
         if (r.P_out) std::memcpy(r.P_out, ws->h_out + (size_t)k * n3, sizeof(double2) * n3 * r.npol);
         if (r.E_out) std::memcpy(r.E_out, ws->h_out + v + (size_t)k * n3, sizeof(double2) * n3 * r.npol);
-        for (int q = 0; q < r.npol; ++q) j->res.info[q] = info[k + q];
+        for (int q = 0; q < r.npol; ++q) j.res.info[q] = info[k + q];
         k += r.npol;
-        j->res.status = TDDA_OK;
-        j->res.batch_rhs = nrhs;
-        j->res.batch_requests = (int)batch.size();
-        j->res.cache_hit = hit ? 1 : 0;
-        j->res.worker = w->id;
-        j->res.queue_ms = ms_between(j->t_submit, j->t_admit);
-        j->res.build_ms = build_ms;
-        j->res.solve_ms = ms_between(ts0, done);
-        j->t_done = Clock::now();
-        j->res.total_ms = ms_between(j->t_submit, j->t_done);
+        j.res.status = TDDA_OK;
+        j.res.batch_rhs = nrhs;
+        j.res.batch_requests = (int)batch.size();
+        j.res.cache_hit = j.hit ? 1 : 0;
+        j.res.worker = w->id;
+        j.res.queue_ms = ms_between(j.t_submit, j.t_admit);
+        j.res.build_ms = build_ms[jj];
+        j.res.solve_ms = ms_between(ts0, done);
+        j.t_done = Clock::now();
+        j.res.total_ms = ms_between(j.t_submit, j.t_done);
     }
 }
 
