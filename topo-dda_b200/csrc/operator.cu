@@ -24,6 +24,7 @@
 #include <vector>
 
 #include "fft_fast.cuh"
+#include "fft_reg.cuh"
 #include "operator.cuh"
 
 namespace tdda {
@@ -151,13 +152,32 @@ __device__ __forceinline__ void fold(int k, int L, int &fk, int &sgn) {
     else { fk = L - k; sgn = -1; }
 }
 
+// The 6 entries of one folded tensor point (xx, xy, xz, yy, yz, zz; 16-byte
+// aligned): three 16-byte loads in complex64, six in complex128.
+template <typename C> __device__ __forceinline__ void load6(const C *__restrict__ a, C (&t)[6]) {
+    if constexpr (sizeof(C) == 8) {
+        const float4 *q = reinterpret_cast<const float4 *>(a);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const float4 v = q[i];
+            t[2 * i].x = v.x; t[2 * i].y = v.y;
+            t[2 * i + 1].x = v.z; t[2 * i + 1].y = v.w;
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < 6; ++i) t[i] = a[i];
+    }
+}
+
 // w (the 3 components of one right-hand side, CKx apart) <- A w for the folded
-// symmetric tensor entry a[6] with the parity signs of its off-diagonal terms
+// symmetric tensor entry a[6], with the parity signs of its off-diagonal terms
 template <typename C>
 __device__ __forceinline__ void mul_sym3(const C *__restrict__ a, typename RealOf<C>::type sxy,
                                          typename RealOf<C>::type sxz, typename RealOf<C>::type syz, C *w, int CKx) {
-    C axx = a[0], axy = sxy * a[1], axz = sxz * a[2];
-    C ayy = a[3], ayz = syz * a[4], azz = a[5];
+    C e[6];
+    load6(a, e);
+    C axx = e[0], axy = sxy * e[1], axz = sxz * e[2];
+    C ayy = e[3], ayz = syz * e[4], azz = e[5];
     C bx = w[0], by = w[CKx], bz = w[2 * CKx];
     w[0] = axx * bx + axy * by + axz * bz;
     w[CKx] = axy * bx + ayy * by + ayz * bz;
@@ -208,9 +228,10 @@ __global__ void __launch_bounds__(NT) k_xconv(ConvGeom g, C *__restrict__ T, con
                 mul_sym3(tab[r] + ti, (R)(sx * sy), (R)(sx * sz), (R)(sy * sz), v + r * 3 * CKx, CKx);
             continue;
         }
-        const C *a = ahat + ti;
-        C axx = a[0], axy = (R)(sx * sy) * a[1], axz = (R)(sx * sz) * a[2];
-        C ayy = a[3], ayz = (R)(sy * sz) * a[4], azz = a[5];
+        C e6[6];
+        load6(ahat + ti, e6);
+        C axx = e6[0], axy = (R)(sx * sy) * e6[1], axz = (R)(sx * sz) * e6[2];
+        C ayy = e6[3], ayz = (R)(sy * sz) * e6[4], azz = e6[5];
         for (int r = 0; r < nrhs; ++r) {
             C *w = v + r * 3 * CKx;
             C bx = w[0], by = w[CKx], bz = w[2 * CKx];
@@ -271,9 +292,10 @@ __global__ void __launch_bounds__(NT2) k_xconv_fast(ConvGeom g, C *__restrict__ 
                 mul_sym3(tab[r] + ti, (R)(sx * sy), (R)(sx * sz), (R)(sy * sz), v + r * 3 * CKx, CKx);
             continue;
         }
-        const C *a = ahat + ti;
-        C axx = a[0], axy = (R)(sx * sy) * a[1], axz = (R)(sx * sz) * a[2];
-        C ayy = a[3], ayz = (R)(sy * sz) * a[4], azz = a[5];
+        C e6[6];
+        load6(ahat + ti, e6);
+        C axx = e6[0], axy = (R)(sx * sy) * e6[1], axz = (R)(sx * sz) * e6[2];
+        C ayy = e6[3], ayz = (R)(sy * sz) * e6[4], azz = e6[5];
         for (int r = 0; r < nrhs; ++r) {
             C *w = v + r * 3 * CKx;
             C bx = w[0], by = w[CKx], bz = w[2 * CKx];
@@ -305,6 +327,152 @@ static bool launch_xconv_fast(const ConvGeom &g, C *T, const C *ahat, const C *c
         default: return false;
     }
 }
+
+// Pass 2 as a register-resident two-level FFT, for Lx = L = R1 * 8 with
+// nx = L / 2 (the zero padding is exactly the upper half):
+//   forward: thread (column, n2) loads x = 8 n1 + n2 (n1 < R1 / 2) straight
+//   from T, runs the half-input R1-point DFT, twiddles by W_L^(n2 k1) and
+//   writes to shared memory; thread (rhs, kz, k1) reads the 8 values of each
+//   of the 3 components, runs 8-point DFTs (X at kx = k1 + R1 k2), applies the
+//   3x3 tensor in registers, runs the inverse 8-point DFTs, twiddles by
+//   W_L^(-n1 k1) and writes back; thread (column, n1) finishes with the
+//   half-output R1-point inverse DFT and stores x = n1 + 8 n2 < nx to T.
+// One shared-memory exchange per direction; every thread holds one task.
+// Tasks run with the kz index fastest, then component / right-hand side, so a
+// half-warp touches consecutive columns of a row (or rows 8 x odd pitch apart):
+// the exchanges are free of bank conflicts.
+constexpr int NTR = 256;
+
+template <typename C, int L>
+__global__ void __launch_bounds__(NTR) k_xconv_reg(ConvGeom g, C *__restrict__ T, const C *__restrict__ ahat,
+                                                   const C *const *__restrict__ tab, const C *__restrict__ tw,
+                                                   int nrhs, const SolverState *__restrict__ st) {
+    using R = typename RealOf<C>::type;
+    constexpr int R2 = 8, R1 = L / R2, H1 = R1 / 2;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *S = reinterpret_cast<C *>(smem_raw);
+    if (st != nullptr) {
+        bool any = false;
+        for (int r = 0; r < nrhs; ++r) any |= (st[r].done == 0);
+        if (!any) return;
+    }
+    const int CK = g.CKr, ky = blockIdx.x, kz0 = blockIdx.y * CK;
+    const int ncol = nrhs * 3 * CK, ncolP = ncol | 1;
+    const size_t plane = (size_t)g.Ly * g.Lz;
+    const size_t off = (size_t)ky * g.Lz + kz0;
+    const int twL = g.Lmax / L, twR1 = g.Lmax / R1;
+    const int t = threadIdx.x;
+    const int tasks1 = ncol * R2, tasks2 = nrhs * CK * R1;
+    // forward, first level: the column's R1-point DFT over x = 8 n1 + n2
+    const int ncomp = nrhs * 3;
+    if (t < tasks1) {
+        const int kl = t % CK, rest = t / CK, rc = rest % ncomp, n2 = rest / ncomp;
+        const int col = rc * CK + kl;
+        const C *src = T + (size_t)rc * g.nx * plane + off + kl;
+        C a[H1], b[H1];
+#pragma unroll
+        for (int n1 = 0; n1 < H1; ++n1) a[n1] = src[(size_t)(R2 * n1 + n2) * plane];
+        dft_half_in<H1, -1>(a, b, tw, twR1);
+#pragma unroll
+        for (int q = 0; q < H1; ++q) {
+            const int k1 = 2 * q;
+            C y0 = a[q], y1 = b[q];
+            if (n2 != 0) {
+                if (k1 != 0) y0 = y0 * twiddle<-1>(tw, n2 * k1 * twL);
+                y1 = y1 * twiddle<-1>(tw, n2 * (k1 + 1) * twL);
+            }
+            S[(k1 * R2 + n2) * ncolP + col] = y0;
+            S[((k1 + 1) * R2 + n2) * ncolP + col] = y1;
+        }
+    }
+    __syncthreads();
+    // second level, tensor, inverse first level
+    C v[3][R2];
+    int kl2 = 0, k1 = 0, rhs = 0;
+    if (t < tasks2) {
+        kl2 = t % CK;
+        const int rest = t / CK;
+        rhs = rest % nrhs;
+        k1 = rest / nrhs;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const int col = (rhs * 3 + c) * CK + kl2;
+#pragma unroll
+            for (int n2 = 0; n2 < R2; ++n2) v[c][n2] = S[(k1 * R2 + n2) * ncolP + col];
+        }
+    }
+    __syncthreads();
+    if (t < tasks2) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) dftR<R2, -1>(v[c]);
+        int fky, sy, fkz, sz;
+        fold(ky, g.Ly, fky, sy);
+        fold(kz0 + kl2, g.Lz, fkz, sz);
+        const C *A = (tab != nullptr) ? tab[rhs] : ahat;
+#pragma unroll
+        for (int k2 = 0; k2 < R2; ++k2) {
+            int fkx, sx;
+            fold(k1 + R1 * k2, L, fkx, sx);
+            C e6[6];
+            load6(A + (((size_t)fky * g.hx + fkx) * g.hz + fkz) * 6, e6);
+            C axx = e6[0], axy = (R)(sx * sy) * e6[1], axz = (R)(sx * sz) * e6[2];
+            C ayy = e6[3], ayz = (R)(sy * sz) * e6[4], azz = e6[5];
+            C bx = v[0][k2], by = v[1][k2], bz = v[2][k2];
+            v[0][k2] = axx * bx + axy * by + axz * bz;
+            v[1][k2] = axy * bx + ayy * by + ayz * bz;
+            v[2][k2] = axz * bx + ayz * by + azz * bz;
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) dftR<R2, +1>(v[c]);
+        if (k1 != 0) {
+#pragma unroll
+            for (int n1 = 1; n1 < R2; ++n1) {
+                const C w = twiddle<+1>(tw, k1 * n1 * twL);
+#pragma unroll
+                for (int c = 0; c < 3; ++c) v[c][n1] = v[c][n1] * w;
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const int col = (rhs * 3 + c) * CK + kl2;
+#pragma unroll
+            for (int n1 = 0; n1 < R2; ++n1) S[(k1 * R2 + n1) * ncolP + col] = v[c][n1];
+        }
+    }
+    __syncthreads();
+    // inverse, second level: outputs x = n1 + 8 n2 for n2 < R1 / 2 (x < nx)
+    if (t < tasks1) {
+        const int kl = t % CK, rest = t / CK, rc = rest % ncomp, n1 = rest / ncomp;
+        const int col = rc * CK + kl;
+        C e[H1], o[H1];
+#pragma unroll
+        for (int q = 0; q < H1; ++q) {
+            e[q] = S[((2 * q) * R2 + n1) * ncolP + col];
+            o[q] = S[((2 * q + 1) * R2 + n1) * ncolP + col];
+        }
+        dft_half_out<H1, +1>(e, o, tw, twR1);
+        C *dst = T + (size_t)rc * g.nx * plane + off + kl;
+#pragma unroll
+        for (int n2 = 0; n2 < H1; ++n2) dst[(size_t)(n1 + R2 * n2) * plane] = e[n2];
+    }
+}
+
+template <typename C>
+static bool launch_xconv_reg(const ConvGeom &g, C *T, const C *ahat, const C *const *tab, const C *tw, int nrhs,
+                             const SolverState *st, cudaStream_t s) {
+    if (!g.reg_x) return false;
+    dim3 grid(g.Ly, g.Lz / g.CKr, 1);
+    switch (g.Lx) {
+        case 256: k_xconv_reg<C, 256><<<grid, NTR, g.smem_r, s>>>(g, T, ahat, tab, tw, nrhs, st); return true;
+        case 192: k_xconv_reg<C, 192><<<grid, NTR, g.smem_r, s>>>(g, T, ahat, tab, tw, nrhs, st); return true;
+        case 128: k_xconv_reg<C, 128><<<grid, NTR, g.smem_r, s>>>(g, T, ahat, tab, tw, nrhs, st); return true;
+        case 96: k_xconv_reg<C, 96><<<grid, NTR, g.smem_r, s>>>(g, T, ahat, tab, tw, nrhs, st); return true;
+        case 64: k_xconv_reg<C, 64><<<grid, NTR, g.smem_r, s>>>(g, T, ahat, tab, tw, nrhs, st); return true;
+        default: return false;
+    }
+}
+
+static bool reg_x_length(int L) { return L == 256 || L == 192 || L == 128 || L == 96 || L == 64; }
 
 static bool fast_x_length(int L) { return L == 256 || L == 192 || L == 128 || L == 96 || L == 64 || L == 32; }
 
@@ -757,6 +925,11 @@ template <typename C> static void set_smem_attrs(int yz, int x) {
     cudaFuncSetAttribute(k_xconv_fast<C, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, x);
     cudaFuncSetAttribute(k_xconv_fast<C, 192>, cudaFuncAttributeMaxDynamicSharedMemorySize, x);
     cudaFuncSetAttribute(k_xconv_fast<C, 96>, cudaFuncAttributeMaxDynamicSharedMemorySize, x);
+    cudaFuncSetAttribute(k_xconv_reg<C, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, x);
+    cudaFuncSetAttribute(k_xconv_reg<C, 192>, cudaFuncAttributeMaxDynamicSharedMemorySize, x);
+    cudaFuncSetAttribute(k_xconv_reg<C, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, x);
+    cudaFuncSetAttribute(k_xconv_reg<C, 96>, cudaFuncAttributeMaxDynamicSharedMemorySize, x);
+    cudaFuncSetAttribute(k_xconv_reg<C, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, x);
     if constexpr (std::is_same<C, float2>::value) {
         // dynamic + static shared memory must stay within the 227 KB opt-in limit;
         // the epilogue kernels carry ~1 KB of static reduction scratch
@@ -831,6 +1004,22 @@ static bool plan_geom(int nx, int ny, int nz, int nrhs, int esize, ConvGeom &g, 
         break;
     }
     if (g.CKx2 == 0 || g.smem_x2 > SMEM_MAX) g.fast_x = 0;
+    // register-resident pass 2: one task per thread at every step
+    g.reg_x = 0;
+    g.CKr = 0;
+    if (reg_x_length(g.Lx) && 2 * nx == g.Lx) {
+        const int R1 = g.Lx / 8;
+        for (int ck = g.Lz; ck >= 1; --ck) {
+            if (g.Lz % ck) continue;
+            const int ncol = nrhs * 3 * ck;
+            const long long bytes = (long long)g.Lx * (ncol | 1) * esize;
+            if (nrhs * ck * R1 > NTR || ncol * 8 > NTR || bytes > SMEM_MAX) continue;
+            g.CKr = ck;
+            g.smem_r = (int)bytes;
+            g.reg_x = 1;
+            break;
+        }
+    }
     return true;
 }
 
@@ -893,7 +1082,8 @@ static tdda_status run_conv(ConvOperator<C> &op, const ConvGeom &g, int nrhs, co
         k_fwd_zy<C, Pro><<<g13, NT, g.smem_yz, s>>>(g, op.T, op.tw, pro);
     dim3 g2(g.Ly, g.Lz / g.CKx, 1);
     count_launches(1);
-    if (!(g.fast_x && launch_xconv_fast<C>(g, op.T, op.ahat, op.ahat_rhs, op.tw, nrhs, st, s)))
+    if (!launch_xconv_reg<C>(g, op.T, op.ahat, op.ahat_rhs, op.tw, nrhs, st, s) &&
+        !(g.fast_x && launch_xconv_fast<C>(g, op.T, op.ahat, op.ahat_rhs, op.tw, nrhs, st, s)))
         k_xconv<C><<<g2, NT, g.smem_x, s>>>(g, op.T, op.ahat, op.ahat_rhs, op.tw, nrhs, st);
     count_launches(1);
     if (!(g.fast_yz && launch_inv_fast<C, Epi>(g, g13, op.T, op.tw, epi, s)))
@@ -1126,7 +1316,8 @@ tdda_status profile_apply(ConvOperator<C> &op, const C *x, C *y, const C *al, in
     });
     ms_pass[1] = timed([&] {
         count_launches(1);
-        if (!(g.fast_x && launch_xconv_fast<C>(g, op.T, op.ahat, op.ahat_rhs, op.tw, nrhs, nullptr, s)))
+        if (!launch_xconv_reg<C>(g, op.T, op.ahat, op.ahat_rhs, op.tw, nrhs, nullptr, s) &&
+            !(g.fast_x && launch_xconv_fast<C>(g, op.T, op.ahat, op.ahat_rhs, op.tw, nrhs, nullptr, s)))
             k_xconv<C><<<g2, NT, g.smem_x, s>>>(g, op.T, op.ahat, op.ahat_rhs, op.tw, nrhs, nullptr);
     });
     ms_pass[2] = timed([&] {

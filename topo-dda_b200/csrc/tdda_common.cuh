@@ -84,6 +84,9 @@ struct ConvGeom {
     long long tcomp;    // nx*Ly*Lz (one component of T)
     int pA;             // SMEM row pitch of the [y][z] slab buffer (elements)
     int YC;             // y columns per z transform call (passes 1 and 3)
+    int reg_x;          // pass 2 on the register-resident two-level FFT
+    int CKr;            // kz chunk of that kernel
+    int smem_r;         // its dynamic SMEM bytes
     int CK;             // kz chunk for the y transforms (passes 1 and 3)
     int pB;             // SMEM row pitch of the [ky][kz-chunk] buffer
     int CKx;            // kz chunk for the x pass (pass 2)
