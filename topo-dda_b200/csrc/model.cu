@@ -614,11 +614,17 @@ static tdda_status update_alpha(tdda_model *m) {
     return TDDA_OK;
 }
 
+// BiCGSTAB iterations per CUDA graph: the solver replays them between polls
+// of the done flags instead of launching their 7 kernels one by one.
+constexpr int kGraphSteps = 4;
+
 static tdda_status solve_c128(tdda_model *m, const double2 *B, double2 *X, int nrhs, bool x0_zero,
                               int max_iter, double tol, tdda_solve_info *info) {
     TRY(ensure_krylov(m, nrhs));
+    KrylovOptions o;
+    o.graph_steps = kGraphSteps;
     return bicgstab_device<double2>(m->op, m->kv, m->al, nullptr, B, X, nrhs, x0_zero, max_iter, tol, m->stream,
-                                    info, KrylovOptions{});
+                                    info, o);
 }
 
 // Refinement workspace of the model, per inner precision.
@@ -648,7 +654,7 @@ static tdda_status solve_refined(tdda_model *m, const double2 *B, double2 *X, in
     w.op64 = &m->op; w.al64 = m->al; w.sc64 = m->precond ? m->sc64 : nullptr;
     w.Rm = m->Rm; w.st_res = m->st_res; w.st_res_host = m->st_res_host;
     w.d_part = m->d_part; w.h_part = m->h_part;
-    w.nbox = m->nbox; w.s = m->stream;
+    w.nbox = m->nbox; w.s = m->stream; w.graph_steps = kGraphSteps;
     return refine_solve<C>(w, B, X, nrhs, x0_zero, max_iter, tol, info);
 }
 

@@ -514,7 +514,21 @@ __global__ void __launch_bounds__(NT3, 1) k_inv_yz_fast(ConvGeom g, const C *__r
     const int x = blockIdx.x, c = blockIdx.y, rhs = blockIdx.z;
     if (epi.skip(rhs)) return;
     const C *Tc = T + ((size_t)(rhs * 3 + c) * g.nx + x) * (size_t)(LY * LZ);
-    for (int e = threadIdx.x; e < LY * LZ; e += NT3) S[(e / LZ) * pS + (e % LZ)] = Tc[e];
+    {
+        // every load of this thread in flight before the first shared-memory store
+        constexpr int NPER = (LY * LZ + NT3 - 1) / NT3;
+        C v[NPER];
+#pragma unroll
+        for (int q = 0; q < NPER; ++q) {
+            const int e = threadIdx.x + q * NT3;
+            if (e < LY * LZ) v[q] = Tc[e];
+        }
+#pragma unroll
+        for (int q = 0; q < NPER; ++q) {
+            const int e = threadIdx.x + q * NT3;
+            if (e < LY * LZ) S[(e / LZ) * pS + (e % LZ)] = v[q];
+        }
+    }
     __syncthreads();
     fft_ip<LY, +1, LZ, NT3>(S, LZ, pS, 1, tw, g.Lmax, LY, g.ny);
     fft_ip<LZ, +1, (LY + 1) / 2, NT3>(S, g.ny, 1, pS, tw, g.Lmax, LZ, g.nz);
