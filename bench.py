@@ -73,6 +73,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving-loop stream")
     ap.add_argument("--small", action="store_true", help="32x32x8, M=5 (quick check, not a bench line)")
+    ap.add_argument("--profile-solve", type=int, default=0, metavar="K",
+                    help="profile case: K mixed-precision solves of the x-polarised RHS, then exit "
+                         "(prints the library's launch count before each, for ncu -s)")
     ap.add_argument("--profile-matvec", type=int, default=0, metavar="K",
                     help="only build the benchmark model and apply the operator K times per precision "
                          "(the case the kernel profiles capture); prints per-pass times")
@@ -286,6 +289,35 @@ def config_block(w, ngpu):
             "l2": "working set > 126 MB L2 (no flush needed)"}
 
 
+def run_periodic_c128(sici):
+    """64x64x16 dipoles, periodic 64d, |m|,|n| <= 50, complex128 throughout: the
+    fused operator's time and algorithmic GB/s, and iterations/s of the
+    reference's BiCGSTAB (unscaled, recursive residual) on it."""
+    import torch
+
+    from dda_model import DDAModel
+
+    w = dict(WORKLOAD, nx=64, ny=64, nz=16, period=64, M=50)
+    kw = model_kwargs(w, sici)
+    m = DDAModel(**kw, precision="complex128")
+    m.setDensities(np.random.default_rng(w["seed"]).random(m.N))
+    ms, passes = m.profile_matvec("complex128", nrhs=1, iters=50)
+    its = 400
+    m.solveElectricField(None, 20, 1e-30)  # warm
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    m.solveElectricField(None, its, 1e-30)
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    done = m.last_solve["iterations"]
+    return {"workload": "64x64x16 dipoles, periodic 64d, |m|,|n|<=50, rho ~ U[0,1] per dipole, complex128, "
+                        "reference BiCGSTAB semantics (no scaling)",
+            "matvec_us": ms * 1e3, "matvec_pass_us": [p * 1e3 for p in passes],
+            "matvec_gbs_algorithmic": 1648.0 * m.N / (ms * 1e-3) / 1e9,
+            "bicgstab_it_per_s": done / dt, "iterations_timed": done,
+            "lattice_ms": m.info["lattice_ms"], "tensor_fft_ms": m.info["tensor_fft_ms"]}
+
+
 def run_serving():
     """The serving workload (see the module docstring) through dda_model.serving."""
     from dda_model.serving import DDAServer, run_stream, synthetic_stream
@@ -342,6 +374,15 @@ def main():
         for prec in ("mixed", "complex128"):
             ms, passes = m.profile_matvec(prec, nrhs=1, iters=args.profile_matvec)
             print(json.dumps({"precision": prec, "ms_matvec": ms, "ms_pass": passes}))
+        return 0
+    if args.profile_solve > 0:
+        m.setPreconditioner("jacobi")
+        P0 = np.zeros(3 * m.N, dtype=np.complex128)
+        for k in range(args.profile_solve):
+            n0 = DDAModel.kernel_launches()
+            m.solveElectricField(P0, MAX_ITER, w["tol"])
+            print(json.dumps({"solve": k, "launches_before": n0, "launches_after": DDAModel.kernel_launches(),
+                              "info": m.last_solve}), flush=True)
         return 0
     N = m.N
     B = torch.from_numpy(np.stack([incident(w, 0), incident(w, 1)])).to(f"cuda:{local}")
@@ -464,6 +505,8 @@ def main():
     serving = None
     if not args.no_serving and not args.small:
         serving = run_serving()
+    periodic = None if args.small else run_periodic_c128((si, ci))
+    log(f"periodic complex128: {periodic}")
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -511,6 +554,7 @@ def main():
             "gpu_launches": int(launches),
             "setup_s": setup_s, "lattice_ms": m.info["lattice_ms"], "tensor_fft_ms": m.info["tensor_fft_ms"],
             "serving": serving,
+            "periodic_c128": periodic,
         }
         print(json.dumps(line))
     if pg:
