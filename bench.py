@@ -203,10 +203,9 @@ def traffic_record():
 
 
 def dist_setup():
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return world, rank, local
+    from dda_model.replicas import env_rank
+
+    return env_rank()
 
 
 # ----------------------------------------------------------------------------
@@ -318,16 +317,25 @@ def run_periodic_c128(sici):
             "lattice_ms": m.info["lattice_ms"], "tensor_fft_ms": m.info["tensor_fft_ms"]}
 
 
-def run_serving():
-    """The serving workload (see the module docstring) through dda_model.serving."""
+def run_serving(rank=0, world=1, device=None):
+    """The serving workload (see the module docstring) through dda_model.serving.
+    With several ranks each serves the requests routed to it by tensor key
+    (replicas; arrival times unchanged), and the throughput is all ranks'
+    requests over the slowest rank's wall time."""
+    from dda_model.replicas import max_over_ranks, shard, sum_over_ranks
     from dda_model.serving import DDAServer, run_stream, synthetic_stream
 
-    reqs = synthetic_stream(n=512, rate=200.0, seed=7)
+    reqs = shard(synthetic_stream(n=512, rate=200.0, seed=7), rank, world)
     with DDAServer(hbm_budget_bytes=120 * 10**9, workers=4, max_rhs=8, use_graphs=True) as srv:
         rep = run_stream(srv, reqs)
         st = srv.stats()
     s = rep.summary()
-    log(f"serving: {s}")
+    log(f"serving (rank {rank}/{world}, {len(reqs)} requests): {s}")
+    wall = max_over_ranks(s["wall_s"], device)
+    nreq = sum_over_ranks(s["requests"], device)
+    s["requests_per_s"] = nreq / wall
+    s["solves_per_s"] = 2 * nreq / wall
+    s["wall_s"] = wall
     return {"workload": "512 requests, Poisson 200 req/s, grids 32x32x8/48x48x12/64x64x16/96x96x16, "
                         "lambda U[450,700] nm, angle U[0,30] deg, 2 RHS each, mixed precision, tol 1e-8, "
                         "120 GB budget, 4 workers, up to 8 RHS per batch",
@@ -429,13 +437,11 @@ def main():
     t_plain, info_plain = timed("complex128", args.steps)
     torch.cuda.synchronize()
 
+    from dda_model.replicas import max_over_ranks
+
     def agg(ts):
-        tot = sum(ts)
-        if pg:
-            t = torch.tensor([tot], device=f"cuda:{local}", dtype=torch.float64)
-            pg.all_reduce(t, op=pg.ReduceOp.MAX)
-            tot = float(t.item())
-        return tot
+        # device-timed region of every rank; the job's time is the slowest rank's
+        return max_over_ranks(sum(ts), f"cuda:{local}")
 
     tot_mixed = agg(t_mixed)
     tot_plain = agg(t_plain)
@@ -476,11 +482,7 @@ def main():
         m.solveElectricField(P0, MAX_ITER, w["tol"])
         E = m.getElectricField()
         te.append(time.perf_counter() - t1)
-    e2e_tot = sum(te)
-    if pg:
-        t = torch.tensor([e2e_tot], device=f"cuda:{local}", dtype=torch.float64)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        e2e_tot = float(t.item())
+    e2e_tot = max_over_ranks(sum(te), f"cuda:{local}")
     e2e = args.steps * world / e2e_tot
     assert np.all(np.isfinite(E))
 
@@ -504,7 +506,7 @@ def main():
 
     serving = None
     if not args.no_serving and not args.small:
-        serving = run_serving()
+        serving = run_serving(rank, world, f"cuda:{local}" if world > 1 else None)
     periodic = None if args.small else run_periodic_c128((si, ci))
     log(f"periodic complex128: {periodic}")
 
