@@ -344,7 +344,7 @@ static bool launch_xconv_fast(const ConvGeom &g, C *T, const C *ahat, const C *c
 constexpr int NTR = 256;
 
 template <typename C, int L>
-__global__ void __launch_bounds__(NTR) k_xconv_reg(ConvGeom g, C *__restrict__ T, const C *__restrict__ ahat,
+__global__ void __launch_bounds__(NTR, sizeof(C) == 8 ? 3 : 1) k_xconv_reg(ConvGeom g, C *__restrict__ T, const C *__restrict__ ahat,
                                                    const C *const *__restrict__ tab, const C *__restrict__ tw,
                                                    int nrhs, const SolverState *__restrict__ st) {
     using R = typename RealOf<C>::type;
