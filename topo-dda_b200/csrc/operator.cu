@@ -589,6 +589,10 @@ static bool launch_inv_fast(const ConvGeom &g, dim3 grid, const C *T, const C *t
     }
 }
 
+}  // namespace tdda
+#include "slab_reg.cuh"
+namespace tdda {
+
 template <typename C, class Epi>
 __global__ void __launch_bounds__(NT) k_inv_yz(ConvGeom g, const C *__restrict__ T,
                                                const C *__restrict__ tw, Epi epi) {
@@ -649,16 +653,20 @@ template <typename C> struct VecBase {
         return (size_t)rhs * dstride + (size_t)cell;
     }
     __device__ __forceinline__ C scaled(int rhs, long long cell, C v) const {
-        return sc != nullptr ? sc[didx(rhs, cell)] * v : v;
+        return sc != nullptr ? __ldg(sc + didx(rhs, cell)) * v : v;
     }
 };
+// Operands that a pass only reads are loaded through the non-coherent path
+// (__ldg): nothing the same kernel stores can alias them (every element is
+// read and written by one thread), so the compiler may issue the loads of
+// several elements ahead of the stores of earlier ones.
 
 template <typename C> struct ProLoad : VecBase<C> {
     const C *x;
     const SolverState *st;  // optional
     __device__ bool skip(int rhs) const { return st != nullptr && st[rhs].done; }
     __device__ C load(int rhs, int c, long long cell) const {
-        return this->scaled(rhs, cell, x[this->idx(rhs, c, cell)]);
+        return this->scaled(rhs, cell, __ldg(x + this->idx(rhs, c, cell)));
     }
 };
 
@@ -672,10 +680,10 @@ template <typename C> struct ProP : VecBase<C> {
     __device__ bool skip(int rhs) const { return st[rhs].done; }
     __device__ C load(int rhs, int c, long long cell) const {
         size_t i = this->idx(rhs, c, cell);
-        C v = r[i];
+        C v = __ldg(r + i);
         if (!first) {
-            C beta = from_d<C>(st[rhs].beta), zeta = from_d<C>(st[rhs].zeta);
-            v = v + beta * (p[i] - zeta * Ap[i]);
+            C beta = from_d<C>(__ldg(&st[rhs].beta)), zeta = from_d<C>(__ldg(&st[rhs].zeta));
+            v = v + beta * (__ldg(p + i) - zeta * __ldg(Ap + i));
         }
         p[i] = v;
         return this->scaled(rhs, cell, v);
@@ -691,8 +699,8 @@ template <typename C> struct ProT : VecBase<C> {
     __device__ bool skip(int rhs) const { return st[rhs].done; }
     __device__ C load(int rhs, int c, long long cell) const {
         size_t i = this->idx(rhs, c, cell);
-        C alpha = from_d<C>(st[rhs].alpha);
-        C v = r[i] - alpha * Ap[i];
+        C alpha = from_d<C>(__ldg(&st[rhs].alpha));
+        C v = __ldg(r + i) - alpha * __ldg(Ap + i);
         t[i] = v;
         return this->scaled(rhs, cell, v);
     }
@@ -704,7 +712,7 @@ template <typename C> struct EpiBase : VecBase<C> {
     unsigned *counter;
     size_t pstride;
     __device__ __forceinline__ C masked(int rhs, long long cell, C conv) const {
-        if (mask != nullptr && mask[cell] == 0) return czero<C>();
+        if (mask != nullptr && __ldg(mask + cell) == 0) return czero<C>();
         return this->scaled(rhs, cell, conv);
     }
 };
@@ -719,7 +727,7 @@ template <typename C> struct EpiMatvec : EpiBase<C> {
     __device__ void apply(int rhs, int c, long long cell, C conv, double2 *) const {
         size_t i = this->idx(rhs, c, cell);
         C v = this->masked(rhs, cell, conv);
-        if (al != nullptr) v = v + al[this->didx(rhs, cell)] * x[i];
+        if (al != nullptr) v = v + __ldg(al + this->didx(rhs, cell)) * __ldg(x + i);
         y[i] = v;
     }
     __device__ void operator()(int, const double2 *) const {}
@@ -734,8 +742,8 @@ template <typename C> struct EpiInit : EpiBase<C> {
     __device__ bool skip(int rhs) const { return false; }
     __device__ void apply(int rhs, int c, long long cell, C conv, double2 *acc) const {
         size_t i = this->idx(rhs, c, cell);
-        C ax = this->masked(rhs, cell, conv) + al[this->didx(rhs, cell)] * x0[i];
-        C bb = b[i];
+        C ax = this->masked(rhs, cell, conv) + __ldg(al + this->didx(rhs, cell)) * __ldg(x0 + i);
+        C bb = __ldg(b + i);
         C v = bb - ax;
         r[i] = v;
         r0[i] = v;
@@ -769,9 +777,9 @@ template <typename C> struct EpiAp : EpiBase<C> {
     __device__ bool skip(int rhs) const { return st[rhs].done; }
     __device__ void apply(int rhs, int c, long long cell, C conv, double2 *acc) const {
         size_t i = this->idx(rhs, c, cell);
-        C v = this->masked(rhs, cell, conv) + al[this->didx(rhs, cell)] * p[i];
+        C v = this->masked(rhs, cell, conv) + __ldg(al + this->didx(rhs, cell)) * __ldg(p + i);
         Ap[i] = v;
-        double2 d = cdot1(to_d(r0[i]), to_d(v));
+        double2 d = cdot1(to_d(__ldg(r0 + i)), to_d(v));
         acc[0].x += d.x;
         acc[0].y += d.y;
     }
@@ -790,8 +798,8 @@ template <typename C> struct EpiAt : EpiBase<C> {
     __device__ bool skip(int rhs) const { return st[rhs].done; }
     __device__ void apply(int rhs, int c, long long cell, C conv, double2 *acc) const {
         size_t i = this->idx(rhs, c, cell);
-        C tv = t[i];
-        C v = this->masked(rhs, cell, conv) + al[this->didx(rhs, cell)] * tv;
+        C tv = __ldg(t + i);
+        C v = this->masked(rhs, cell, conv) + __ldg(al + this->didx(rhs, cell)) * tv;
         At[i] = v;
         double2 vd = to_d(v);
         double2 d = cdot1(vd, to_d(tv));
@@ -866,12 +874,12 @@ __global__ void __launch_bounds__(NT) k_update(long long n, C *__restrict__ P, c
     double2 acc[2] = {make_double2(0.0, 0.0), make_double2(0.0, 0.0)};
     for (long long i = (long long)blockIdx.x * NT + threadIdx.x; i < n; i += (long long)gridDim.x * NT) {
         size_t k = base + i;
-        C tv = t[k];
-        P[k] = P[k] + alpha * p[k] + zeta * tv;
-        C rn = tv - zeta * At[k];
+        C tv = __ldg(t + k);
+        P[k] = P[k] + alpha * __ldg(p + k) + zeta * tv;
+        C rn = tv - zeta * __ldg(At + k);
         r[k] = rn;
         double2 rd = to_d(rn);
-        double2 d = cdot1(to_d(r0[k]), rd);
+        double2 d = cdot1(to_d(__ldg(r0 + k)), rd);
         acc[0].x += d.x;
         acc[0].y += d.y;
         acc[1].x += rd.x * rd.x + rd.y * rd.y;
@@ -957,6 +965,16 @@ template <typename C> static void set_smem_attrs(int yz, int x) {
     cudaFuncSetAttribute(k_inv_yz_fast<C, a, b, EpiAt<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemFast);
         TDDA_YZ_PAIRS(TDDA_ATTR)
 #undef TDDA_ATTR
+#define TDDA_ATTR_REG(a, b)                                                                                          \
+    cudaFuncSetAttribute(k_fwd_zy_reg<C, a, b, ProLoad<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemFast);    \
+    cudaFuncSetAttribute(k_fwd_zy_reg<C, a, b, ProP<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemFast);       \
+    cudaFuncSetAttribute(k_fwd_zy_reg<C, a, b, ProT<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemFast);       \
+    cudaFuncSetAttribute(k_inv_yz_reg<C, a, b, EpiMatvec<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemFast);  \
+    cudaFuncSetAttribute(k_inv_yz_reg<C, a, b, EpiInit<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemFast);    \
+    cudaFuncSetAttribute(k_inv_yz_reg<C, a, b, EpiAp<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemFast);      \
+    cudaFuncSetAttribute(k_inv_yz_reg<C, a, b, EpiAt<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemFast);
+        TDDA_YZ_REG_PAIRS(TDDA_ATTR_REG)
+#undef TDDA_ATTR_REG
     }
     cudaGetLastError();  // a refused opt-in shows up at launch time, not here
 }
@@ -1005,6 +1023,13 @@ static bool plan_geom(int nx, int ny, int nz, int nrhs, int esize, ConvGeom &g, 
     // compile-time slab kernels for passes 1 and 3 (complex64 only)
     g.smem_yz2 = (int)((long long)g.Ly * (g.Lz + 1) * esize);
     g.fast_yz = (esize == 8 && fast_yz_pair(g.Lz, g.Ly) && g.smem_yz2 <= kSmemFast) ? 1 : 0;
+    // register two-level slab kernels: half padding on both axes
+    g.reg_yz = 0;
+    if (esize == 8 && 2 * ny == g.Ly && 2 * nz == g.Lz && reg_yz_pair(g.Lz, g.Ly)) {
+        g.smem_fr = slab_reg_smem(ny, g.Lz, g.Ly, true, esize);
+        g.smem_ir = slab_reg_smem(ny, g.Lz, g.Ly, false, esize);
+        g.reg_yz = (g.smem_fr <= kSmemFast && g.smem_ir <= kSmemFast) ? 1 : 0;
+    }
     // compile-time-length pass 2: two ping-pong buffers, at most ~100 KB so
     // that two CTAs share an SM; runs of >= 64 bytes along kz
     g.fast_x = fast_x_length(g.Lx) ? 1 : 0;
@@ -1092,7 +1117,8 @@ static tdda_status run_conv(ConvOperator<C> &op, const ConvGeom &g, int nrhs, co
                             const Epi &epi, const SolverState *st, cudaStream_t s) {
     dim3 g13(g.nx, 3, nrhs);
     count_launches(1);
-    if (!(g.fast_yz && launch_fwd_fast<C, Pro>(g, g13, op.T, op.tw, pro, s)))
+    if (!launch_fwd_reg<C, Pro>(g, g13, op.T, op.tw, pro, s) &&
+        !(g.fast_yz && launch_fwd_fast<C, Pro>(g, g13, op.T, op.tw, pro, s)))
         k_fwd_zy<C, Pro><<<g13, NT, g.smem_yz, s>>>(g, op.T, op.tw, pro);
     dim3 g2(g.Ly, g.Lz / g.CKx, 1);
     count_launches(1);
@@ -1100,7 +1126,8 @@ static tdda_status run_conv(ConvOperator<C> &op, const ConvGeom &g, int nrhs, co
         !(g.fast_x && launch_xconv_fast<C>(g, op.T, op.ahat, op.ahat_rhs, op.tw, nrhs, st, s)))
         k_xconv<C><<<g2, NT, g.smem_x, s>>>(g, op.T, op.ahat, op.ahat_rhs, op.tw, nrhs, st);
     count_launches(1);
-    if (!(g.fast_yz && launch_inv_fast<C, Epi>(g, g13, op.T, op.tw, epi, s)))
+    if (!launch_inv_reg<C, Epi>(g, g13, op.T, op.tw, epi, s) &&
+        !(g.fast_yz && launch_inv_fast<C, Epi>(g, g13, op.T, op.tw, epi, s)))
         k_inv_yz<C, Epi><<<g13, NT, g.smem_yz, s>>>(g, op.T, op.tw, epi);
     return TDDA_OK;
 }
@@ -1325,7 +1352,8 @@ tdda_status profile_apply(ConvOperator<C> &op, const C *x, C *y, const C *al, in
     *ms_total = timed([&] { run_conv(op, g, nrhs, pro, epi, nullptr, s); });
     ms_pass[0] = timed([&] {
         count_launches(1);
-        if (!(g.fast_yz && launch_fwd_fast<C, ProLoad<C>>(g, g13, op.T, op.tw, pro, s)))
+        if (!launch_fwd_reg<C, ProLoad<C>>(g, g13, op.T, op.tw, pro, s) &&
+            !(g.fast_yz && launch_fwd_fast<C, ProLoad<C>>(g, g13, op.T, op.tw, pro, s)))
             k_fwd_zy<C, ProLoad<C>><<<g13, NT, g.smem_yz, s>>>(g, op.T, op.tw, pro);
     });
     ms_pass[1] = timed([&] {
@@ -1336,7 +1364,8 @@ tdda_status profile_apply(ConvOperator<C> &op, const C *x, C *y, const C *al, in
     });
     ms_pass[2] = timed([&] {
         count_launches(1);
-        if (!(g.fast_yz && launch_inv_fast<C, EpiMatvec<C>>(g, g13, op.T, op.tw, epi, s)))
+        if (!launch_inv_reg<C, EpiMatvec<C>>(g, g13, op.T, op.tw, epi, s) &&
+            !(g.fast_yz && launch_inv_fast<C, EpiMatvec<C>>(g, g13, op.T, op.tw, epi, s)))
             k_inv_yz<C, EpiMatvec<C>><<<g13, NT, g.smem_yz, s>>>(g, op.T, op.tw, epi);
     });
     cudaEventDestroy(e0);

@@ -87,6 +87,8 @@ struct ConvGeom {
     int reg_x;          // pass 2 on the register-resident two-level FFT
     int CKr;            // kz chunk of that kernel
     int smem_r;         // its dynamic SMEM bytes
+    int reg_yz;         // passes 1 and 3 on the register two-level slab kernels
+    int smem_fr, smem_ir;  // their dynamic SMEM bytes (forward, inverse)
     int CK;             // kz chunk for the y transforms (passes 1 and 3)
     int pB;             // SMEM row pitch of the [ky][kz-chunk] buffer
     int CKx;            // kz chunk for the x pass (pass 2)
