@@ -120,6 +120,9 @@ tdda_status tdda_calculate_gradients(tdda_model *m, double epsilon_partial, doub
 tdda_status tdda_set_parameters(tdda_model *m, const double *values, int64_t n);
 /* DDAModel::get_parameter_copy (src/DDAModel.cpp:1341-1343; binding :67) */
 tdda_status tdda_get_parameters(const tdda_model *m, double *out, int64_t n);
+/* The dipole -> parameter map of src/DDAModel.cpp:163-247 (geometryPara):
+ * map[i] is the free parameter that sets dipole i's density; int32[N]. */
+tdda_status tdda_get_parameter_map(const tdda_model *m, int32_t *map, int64_t n);
 /* DDAModel::get_dielectrics_copy (src/DDAModel.cpp:1346-1348; binding :68): double[3N] */
 tdda_status tdda_get_dielectrics(const tdda_model *m, double *out, int64_t n);
 /* DDAModel::get_EResult (src/DDAModel.cpp:1254-1256; binding :69): complex[3N] */

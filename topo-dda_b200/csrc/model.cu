@@ -1025,6 +1025,13 @@ tdda_status tdda_get_parameters(const tdda_model *m, double *out, int64_t n) {
     return TDDA_OK;
 }
 
+tdda_status tdda_get_parameter_map(const tdda_model *m, int32_t *map, int64_t n) {
+    if (!m || !map) return bad("null argument");
+    if (n != m->N) return bad("map buffer must hold num_total entries");
+    for (int i = 0; i < m->N; ++i) map[i] = m->geometryPara[i];
+    return TDDA_OK;
+}
+
 tdda_status tdda_get_dielectrics(const tdda_model *m, double *out, int64_t n) {
     if (!m || !out) return bad("null argument");
     if (n != 3LL * m->N) return bad("buffer must hold 3N values");

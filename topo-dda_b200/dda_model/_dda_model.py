@@ -147,6 +147,13 @@ class DDAModel:
         _lib.check(self._lib.tdda_get_parameters(self._handle, _dp(g), g.size))
         return g
 
+    def parameterMap(self):
+        """Free parameter of every dipole (src/DDAModel.cpp:163-247), int32[N]."""
+        out = np.zeros(self.N, dtype=np.int32)
+        _lib.check(self._lib.tdda_get_parameter_map(self._handle, out.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                                                    out.size))
+        return out
+
     def getDielectrics(self):
         g = np.zeros(3 * self.N)
         _lib.check(self._lib.tdda_get_dielectrics(self._handle, _dp(g), g.size))

@@ -153,6 +153,7 @@ SIGNATURES = {
                                                 ctypes.c_int, ctypes.c_double, _dp, ctypes.c_int64]),
     "tdda_set_parameters": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_int64]),
     "tdda_get_parameters": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_int64]),
+    "tdda_get_parameter_map": (ctypes.c_int, [ctypes.c_void_p, _ip, ctypes.c_int64]),
     "tdda_get_dielectrics": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_int64]),
     "tdda_get_electric_field": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_int64]),
     "tdda_get_polarization": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_int64]),
