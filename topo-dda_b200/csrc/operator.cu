@@ -1017,7 +1017,8 @@ static bool plan_geom(int nx, int ny, int nz, int nrhs, int esize, ConvGeom &g, 
         g.CKx = ck;
         break;
     }
-    if (g.CKx == 0) { why = "x pencils do not fit in shared memory"; return false; }
+    // (CKx == 0: the generic x pass cannot hold this batch; a compile-time
+    // x pass below may still take it)
     g.pC = nrhs * 3 * g.CKx;
     g.smem_x = g.Lx * g.pC * esize;
     // compile-time slab kernels for passes 1 and 3 (complex64 only)
@@ -1059,6 +1060,7 @@ static bool plan_geom(int nx, int ny, int nz, int nrhs, int esize, ConvGeom &g, 
             break;
         }
     }
+    if (g.CKx == 0 && !g.fast_x && !g.reg_x) { why = "x pencils do not fit in shared memory"; return false; }
     return true;
 }
 
@@ -1120,7 +1122,7 @@ static tdda_status run_conv(ConvOperator<C> &op, const ConvGeom &g, int nrhs, co
     if (!launch_fwd_reg<C, Pro>(g, g13, op.T, op.tw, pro, s) &&
         !(g.fast_yz && launch_fwd_fast<C, Pro>(g, g13, op.T, op.tw, pro, s)))
         k_fwd_zy<C, Pro><<<g13, NT, g.smem_yz, s>>>(g, op.T, op.tw, pro);
-    dim3 g2(g.Ly, g.Lz / g.CKx, 1);
+    dim3 g2(g.Ly, g.CKx > 0 ? g.Lz / g.CKx : 1, 1);
     count_launches(1);
     if (!launch_xconv_reg<C>(g, op.T, op.ahat, op.ahat_rhs, op.tw, nrhs, st, s) &&
         !(g.fast_x && launch_xconv_fast<C>(g, op.T, op.ahat, op.ahat_rhs, op.tw, nrhs, st, s)))
@@ -1338,7 +1340,7 @@ tdda_status profile_apply(ConvOperator<C> &op, const C *x, C *y, const C *al, in
     cudaEvent_t e0, e1;
     TDDA_CUDA_TRY(cudaEventCreate(&e0));
     TDDA_CUDA_TRY(cudaEventCreate(&e1));
-    dim3 g13(g.nx, 3, nrhs), g2(g.Ly, g.Lz / g.CKx, 1);
+    dim3 g13(g.nx, 3, nrhs), g2(g.Ly, g.CKx > 0 ? g.Lz / g.CKx : 1, 1);
     auto timed = [&](auto &&fn) -> double {
         fn();  // warm
         cudaEventRecord(e0, s);
