@@ -183,3 +183,53 @@ def test_stream_of_mixed_requests(sici):
     assert s["max_true_error"] <= 1e-8
     assert s["p99_ms"] >= s["p50_ms"] > 0
     assert st["completed"] == 24 and st["failed"] == 0
+
+
+def test_invalid_requests_and_tickets(sici):
+    """Bad requests fail at submit with a message; unknown tickets and
+    timeouts are reported, not waited on forever."""
+    import ctypes
+
+    from dda_model import TddaError, _lib
+    from dda_model.serving import Request
+
+    with _server(sici=sici, workers=1) as srv:
+        good = _request((8, 8, 4), seed=60)
+        bad = [
+            Request(shape=(8, 8, 4), rho=np.full(256, 1.5)),                        # density outside [0, 1]
+            Request(shape=(8, 8, 4), rho=np.zeros(256), polarisations=((1, 0, 0),) * 5),  # > 4 polarisations
+            Request(shape=(8, 8, 4), rho=np.zeros(256), tol=0.0),
+            Request(shape=(8, 8, 4), rho=np.zeros(256), lam=-1.0),
+        ]
+        for r in bad:
+            with pytest.raises((TddaError, ValueError, IndexError)):
+                srv.submit(r)
+        with pytest.raises(ValueError):
+            srv.submit(Request(shape=(8, 8, 4), rho=np.zeros(10)))             # wrong size
+        res = _lib.RequestResult()
+        assert srv._lib.tdda_server_wait(srv._h, 987654, 0.0, ctypes.byref(res)) == 1  # unknown ticket
+        t = srv.submit(good)
+        out = srv.wait(t)
+        assert out.info[0]["status"] == "converged"
+        assert srv._lib.tdda_server_wait(srv._h, t, 0.0, ctypes.byref(res)) == 1       # waited for once
+        st = srv.stats()
+        assert st["submitted"] == 1 and st["completed"] == 1 and st["failed"] == 0
+
+
+def test_shutdown_finishes_queued_work(sici):
+    """Closing the server with requests still queued finishes them first (their
+    output buffers are filled) and then returns."""
+    import ctypes
+
+    from dda_model import _lib
+    from dda_model.serving import DDAServer
+
+    srv = DDAServer(hbm_budget_bytes=8 * 10**9, workers=1, sici=sici)
+    reqs = [_request((12, 12, 4), seed=70 + i, lam=500.0 + 20 * i) for i in range(4)]
+    tickets = [srv.submit(r) for r in reqs]
+    # a zero timeout on the last request, which cannot have finished yet, reports TIMEOUT
+    res = _lib.RequestResult()
+    assert srv._lib.tdda_server_wait(srv._h, tickets[-1], 0.0, ctypes.byref(res)) in (0, 6)
+    outputs = [srv._pending[t][1] for t in tickets]
+    srv.close()
+    assert all(np.abs(P).max() > 0 for P in outputs)
