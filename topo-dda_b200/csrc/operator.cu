@@ -67,6 +67,10 @@ template <int NQ> __device__ __forceinline__ void block_sum(double2 (&v)[NQ]) {
 
 // Every block contributes NQ complex sums; the last block to finish adds the
 // per-block partials in block order and calls fin(rhs, totals) on thread 0.
+// The partials of one RHS take nblk * NQ entries: the scratch holds
+// max(3 nx, UPD_BLOCKS) * kMaxNQ per RHS (pass 3 runs nx * 3 blocks per RHS,
+// the vector kernels UPD_BLOCKS), and no reduction uses more than kMaxNQ sums.
+constexpr int kMaxNQ = 4;
 template <int NQ, class Fin>
 __device__ __forceinline__ void reduce_finalize(double2 (&v)[NQ], double2 *part, unsigned *counter,
                                                 int bid, int nblk, const Fin &fin, int rhs) {
@@ -816,13 +820,45 @@ template <typename C> struct EpiAt : EpiBase<C> {
 };
 
 // Finalize after the P/r update: bookkeeping of src/DDAModel.cpp:940-1008.
-struct FinUpdate {
+// Fused variant of the At epilogue: also r0.t, r0.At and ||t||^2, from which
+// the finalize forms the next recursive residual without the update pass:
+//   r = t - zeta At,  r0.r = r0.t - zeta r0.At,
+//   ||r||^2 = ||t||^2 - 2 Re(conj(zeta) <At, t>) + |zeta|^2 ||At||^2
+// (FP64 sums; the vectors r and P are formed by the next iteration's first
+// pass, ProPF, or by k_flush after the last iteration).
+template <typename C> struct EpiAtF : EpiBase<C> {
+    static constexpr int NQ = 4;
+    static_assert(NQ <= kMaxNQ, "reduction scratch holds kMaxNQ sums per block");
+    const C *t, *al, *r0;
+    C *At;
     SolverState *st;
-    __device__ void operator()(int rhs, const double2 *s) const {
-        SolverState &S = st[rhs];
+    __device__ bool skip(int rhs) const { return st[rhs].done; }
+    __device__ void apply(int rhs, int c, long long cell, C conv, double2 *acc) const {
+        size_t i = this->idx(rhs, c, cell);
+        const C tv = __ldg(t + i);
+        const C v = this->masked(rhs, cell, conv) + __ldg(al + this->didx(rhs, cell)) * tv;
+        At[i] = v;
+        const double2 vd = to_d(v), td = to_d(tv), r0d = to_d(__ldg(r0 + i));
+        const double2 d0 = cdot1(vd, td);
+        acc[0].x += d0.x;
+        acc[0].y += d0.y;
+        acc[1].x += vd.x * vd.x + vd.y * vd.y;
+        acc[1].y += td.x * td.x + td.y * td.y;
+        const double2 d2 = cdot1(r0d, td), d3 = cdot1(r0d, vd);
+        acc[2].x += d2.x;
+        acc[2].y += d2.y;
+        acc[3].x += d3.x;
+        acc[3].y += d3.y;
+    }
+    __device__ void operator()(int rhs, const double2 *s) const;
+};
+
+// One loop pass's bookkeeping after the new r: stopping tests and beta.
+__device__ __forceinline__ void finish_iteration(SolverState &S, double2 rho_new, double rnorm2) {
+    {
         S.rho_prev = S.rho;
-        S.rho = s[0];
-        S.err = sqrt(s[1].x) / S.enorm;
+        S.rho = rho_new;
+        S.err = sqrt(rnorm2) / S.enorm;
         const int it = S.it;
         if (S.stall_limit > 0 && it >= 0 && S.err < 0.9 * S.best_err) {
             S.best_err = S.err;
@@ -856,7 +892,68 @@ struct FinUpdate {
         }
         S.it = it + 1;
     }
+}
+
+struct FinUpdate {
+    SolverState *st;
+    __device__ void operator()(int rhs, const double2 *s) const { finish_iteration(st[rhs], s[0], s[1].x); }
 };
+
+template <typename C> __device__ void EpiAtF<C>::operator()(int rhs, const double2 *s) const {
+    SolverState &S = st[rhs];
+    const double2 atat = make_double2(s[1].x, 0.0);
+    S.zeta = cdiv(s[0], atat);
+    const double2 z = S.zeta;
+    // Re(conj(zeta) <At,t>) and |zeta|^2
+    const double re = z.x * s[0].x + z.y * s[0].y;
+    const double z2 = z.x * z.x + z.y * z.y;
+    const double rn2 = fmax(s[1].y - 2.0 * re + z2 * s[1].x, 0.0);
+    const double2 rho_new = make_double2(s[2].x - (z.x * s[3].x - z.y * s[3].y),
+                                         s[2].y - (z.x * s[3].y + z.y * s[3].x));
+    S.pending = 1;
+    finish_iteration(S, rho_new, rn2);
+}
+
+// Fused first pass: the previous iteration's r = t - zeta At and
+// P += alpha p + zeta t, then p = r + beta (p - zeta Ap)  (first step: p = r)
+template <typename C> struct ProPF : VecBase<C> {
+    C *r, *P, *p;
+    const C *t, *At, *Ap;
+    const SolverState *st;
+    int first;
+    __device__ bool skip(int rhs) const { return st[rhs].done; }
+    __device__ C load(int rhs, int c, long long cell) const {
+        const size_t i = this->idx(rhs, c, cell);
+        C v;
+        if (first) {
+            v = __ldg(r + i);
+        } else {
+            const C alpha = from_d<C>(__ldg(&st[rhs].alpha)), zeta = from_d<C>(__ldg(&st[rhs].zeta));
+            const C beta = from_d<C>(__ldg(&st[rhs].beta));
+            const C tv = __ldg(t + i), pv = __ldg(p + i);
+            const C rn = tv - zeta * __ldg(At + i);
+            r[i] = rn;
+            P[i] = P[i] + alpha * pv + zeta * tv;
+            v = rn + beta * (pv - zeta * __ldg(Ap + i));
+        }
+        p[i] = v;
+        return this->scaled(rhs, cell, v);
+    }
+};
+
+// After a fused solve: the last iteration's P += alpha p + zeta t
+template <typename C>
+__global__ void __launch_bounds__(NT) k_flush(long long n, C *__restrict__ P, const C *__restrict__ p,
+                                              const C *__restrict__ t, const SolverState *st) {
+    const int rhs = blockIdx.y;
+    if (!st[rhs].pending) return;
+    const C alpha = from_d<C>(st[rhs].alpha), zeta = from_d<C>(st[rhs].zeta);
+    const size_t base = (size_t)rhs * n;
+    for (long long i = (long long)blockIdx.x * NT + threadIdx.x; i < n; i += (long long)gridDim.x * NT) {
+        const size_t k = base + i;
+        P[k] = P[k] + alpha * __ldg(p + k) + zeta * __ldg(t + k);
+    }
+}
 
 // P += alpha p + zeta t;  r = t - zeta At;  sums r0.r, ||r||^2
 // (src/DDAModel.cpp:937-941,980-984, with alpha p + zeta r - alpha zeta Ap
@@ -936,6 +1033,8 @@ template <typename C> static void set_smem_attrs(int yz, int x) {
     cudaFuncSetAttribute(k_fwd_zy<C, ProLoad<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, yz);
     cudaFuncSetAttribute(k_fwd_zy<C, ProP<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, yz);
     cudaFuncSetAttribute(k_fwd_zy<C, ProT<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, yz);
+    cudaFuncSetAttribute(k_fwd_zy<C, ProPF<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, yz);
+    cudaFuncSetAttribute(k_inv_yz<C, EpiAtF<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, yz);
     cudaFuncSetAttribute(k_inv_yz<C, EpiMatvec<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, yz);
     cudaFuncSetAttribute(k_inv_yz<C, EpiInit<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, yz);
     cudaFuncSetAttribute(k_inv_yz<C, EpiAp<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, yz);
@@ -959,6 +1058,8 @@ template <typename C> static void set_smem_attrs(int yz, int x) {
     cudaFuncSetAttribute(k_fwd_zy_fast<C, a, b, ProLoad<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemFast);   \
     cudaFuncSetAttribute(k_fwd_zy_fast<C, a, b, ProP<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemFast);      \
     cudaFuncSetAttribute(k_fwd_zy_fast<C, a, b, ProT<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemFast);      \
+    cudaFuncSetAttribute(k_fwd_zy_fast<C, a, b, ProPF<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemFast);     \
+    cudaFuncSetAttribute(k_inv_yz_fast<C, a, b, EpiAtF<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemFast);    \
     cudaFuncSetAttribute(k_inv_yz_fast<C, a, b, EpiMatvec<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemFast); \
     cudaFuncSetAttribute(k_inv_yz_fast<C, a, b, EpiInit<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemFast);   \
     cudaFuncSetAttribute(k_inv_yz_fast<C, a, b, EpiAp<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemFast);     \
@@ -969,6 +1070,8 @@ template <typename C> static void set_smem_attrs(int yz, int x) {
     cudaFuncSetAttribute(k_fwd_zy_reg<C, a, b, ProLoad<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemFast);    \
     cudaFuncSetAttribute(k_fwd_zy_reg<C, a, b, ProP<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemFast);       \
     cudaFuncSetAttribute(k_fwd_zy_reg<C, a, b, ProT<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemFast);       \
+    cudaFuncSetAttribute(k_fwd_zy_reg<C, a, b, ProPF<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemFast);      \
+    cudaFuncSetAttribute(k_inv_yz_reg<C, a, b, EpiAtF<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemFast);     \
     cudaFuncSetAttribute(k_inv_yz_reg<C, a, b, EpiMatvec<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemFast);  \
     cudaFuncSetAttribute(k_inv_yz_reg<C, a, b, EpiInit<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemFast);    \
     cudaFuncSetAttribute(k_inv_yz_reg<C, a, b, EpiAp<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemFast);      \
@@ -1082,7 +1185,7 @@ template <typename C> tdda_status ConvOperator<C>::init(int nx, int ny, int nz, 
     TDDA_CUDA_TRY(cudaMalloc(&tw, sizeof(C) * g.Lmax));
     TDDA_CUDA_TRY(cudaMemcpy(tw, h.data(), sizeof(C) * g.Lmax, cudaMemcpyHostToDevice));
     TDDA_CUDA_TRY(cudaMalloc(&T, sizeof(C) * (size_t)nrhs_cap * 3 * g.tcomp));
-    partial_cap = std::max(3 * nx, UPD_BLOCKS) * 2;
+    partial_cap = std::max(3 * nx, UPD_BLOCKS) * kMaxNQ;
     TDDA_CUDA_TRY(cudaMalloc(&partials, sizeof(double2) * (size_t)partial_cap * nrhs_cap));
     TDDA_CUDA_TRY(cudaMalloc(&counters, sizeof(unsigned) * (size_t)nrhs_cap));
     TDDA_CUDA_TRY(cudaMemset(counters, 0, sizeof(unsigned) * (size_t)nrhs_cap));
@@ -1093,7 +1196,7 @@ size_t conv_workspace_bytes(int nx, int ny, int nz, int nrhs_cap, int esize) {
     ConvGeom g;
     std::string why;
     if (!plan_geom(nx, ny, nz, 1, esize, g, why)) return 0;
-    const size_t partial_cap = (size_t)std::max(3 * nx, UPD_BLOCKS) * 2;
+    const size_t partial_cap = (size_t)std::max(3 * nx, UPD_BLOCKS) * kMaxNQ;
     return (size_t)esize * g.Lmax + (size_t)esize * nrhs_cap * 3 * g.tcomp + sizeof(double2) * partial_cap * nrhs_cap +
            sizeof(unsigned) * nrhs_cap;
 }
@@ -1222,9 +1325,32 @@ tdda_status bicgstab_device(ConvOperator<C> &op, Krylov<C> &kv, const C *al, con
     }
     TDDA_CUDA_TRY(cudaGetLastError());
 
-    // one BiCGSTAB step: Ap, alpha, t, At, zeta, P/r update, beta (7 launches)
-    constexpr int kLaunchesPerStep = 7;
+    // one BiCGSTAB step: Ap, alpha, t, At, zeta, P/r update, beta (7 launches;
+    // 6 fused, the P/r update riding in the next step's first pass)
+    const int kLaunchesPerStep = o.fused ? 6 : 7;
+    auto step_fused = [&](bool first) {
+        ProPF<C> pp{};
+        pp.nbox = g.nbox; pp.r = kv.r; pp.P = X; pp.p = kv.p; pp.t = kv.t; pp.At = kv.At; pp.Ap = kv.Ap;
+        pp.st = kv.st; pp.first = first ? 1 : 0; pp.sc = sc; pp.dstride = o.dstride;
+        EpiAp<C> ea{};
+        ea.nbox = g.nbox; ea.mask = op.mask; ea.part = op.partials; ea.counter = op.counters; ea.pstride = ps;
+        ea.p = kv.p; ea.al = al; ea.r0 = kv.r0; ea.Ap = kv.Ap; ea.st = kv.st;
+        ea.sc = sc; ea.dstride = o.dstride;
+        run_conv(op, g, nrhs, pp, ea, kv.st, s);
+        ProT<C> pt{};
+        pt.nbox = g.nbox; pt.r = kv.r; pt.Ap = kv.Ap; pt.t = kv.t; pt.st = kv.st;
+        pt.sc = sc; pt.dstride = o.dstride;
+        EpiAtF<C> et{};
+        et.nbox = g.nbox; et.mask = op.mask; et.part = op.partials; et.counter = op.counters; et.pstride = ps;
+        et.t = kv.t; et.al = al; et.r0 = kv.r0; et.At = kv.At; et.st = kv.st;
+        et.sc = sc; et.dstride = o.dstride;
+        run_conv(op, g, nrhs, pt, et, kv.st, s);
+    };
     auto step = [&](bool first) {
+        if (o.fused) {
+            step_fused(first);
+            return;
+        }
         ProP<C> pp{};
         pp.nbox = g.nbox; pp.r = kv.r; pp.p = kv.p; pp.Ap = kv.Ap; pp.st = kv.st; pp.first = first ? 1 : 0;
         pp.sc = sc; pp.dstride = o.dstride;
@@ -1302,6 +1428,12 @@ tdda_status bicgstab_device(ConvOperator<C> &op, Krylov<C> &kv, const C *al, con
             return TDDA_ERR_STATE;
         }
         chunk = std::min(chunk * 2, 16);
+    }
+    if (o.fused) {
+        dim3 gu(UPD_BLOCKS, nrhs);
+        count_launches(1);
+        k_flush<C><<<gu, NT, 0, s>>>(n, X, kv.p, kv.t, kv.st);
+        TDDA_CUDA_TRY(cudaGetLastError());
     }
     if (info != nullptr)
         for (int k = 0; k < nrhs; ++k) {

@@ -23,6 +23,8 @@ struct SolverState {
     int stall_limit;    // >0: stop when err has not dropped 10% in this many iterations
     int best_it;
     double best_err;
+    int pending;        // fused steps: the last iteration's P update is not applied yet
+    int pad_;
 };
 
 // Geometry + device buffers of one operator instance (one precision).
@@ -68,6 +70,9 @@ struct KrylovOptions {
                                    // iterations without a 10% drop of the residual
     size_t dstride = 0;            // diagonal (al, sc) per rhs at [rhs][cell] when nbox, shared when 0
     int graph_steps = 0;           // > 0: capture this many iterations in a CUDA graph and replay it
+    bool fused = false;            // fold the P/r update into the next iteration's first pass
+                                   // (recursive residual norm from dot products; not the
+                                   // reference's exact bookkeeping)
 };
 
 // BiCGSTAB of DDAModel::bicgstab on the fused operator: solves

@@ -123,6 +123,7 @@ tdda_status refine_solve(const RefineWork<C> &w, const double2 *B, double2 *X, i
         o.stall_limit = kInnerStall;
         o.dstride = w.dstride;
         o.graph_steps = w.graph_steps;
+        o.fused = true;
         st = bicgstab_device<C>(*w.op, *w.kv, w.al, w.sc, w.R, w.D, nrhs, true, budget, h[2 * nrhs], s, ii.data(), o);
         if (st != TDDA_OK) return st;
         launch_axpy_inner<C>(n, w.nbox, nrhs, w.dstride, w.d_part + nrhs, w.sc64, w.D, X, s);
