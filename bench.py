@@ -31,8 +31,9 @@ The line also carries "serving": the request loop of dda_model.serving on
 mixed precision to a 1e-8 true residual under a 120 GB admission budget
 (latency = result ready - submit, wall-clock; throughput over the whole
 stream), and "serving.below_capacity": 256 requests of the same mix at 30
-req/s, where latency is service time rather than queueing.  --no-serving
-skips both.
+req/s, where latency is service time rather than queueing.  Both servers
+allocate their workspaces for the four grids before the stream starts.
+--no-serving skips both.
 """
 from __future__ import annotations
 
@@ -327,8 +328,12 @@ def run_serving(rank=0, world=1, device=None):
     from dda_model.replicas import max_over_ranks, shard, sum_over_ranks
     from dda_model.serving import DDAServer, run_stream, synthetic_stream
 
+    from dda_model.serving import SERVE_SHAPES
+
     reqs = shard(synthetic_stream(n=512, rate=200.0, seed=7), rank, world)
     with DDAServer(hbm_budget_bytes=120 * 10**9, workers=4, max_rhs=8, use_graphs=True) as srv:
+        for shape in SERVE_SHAPES:   # workspaces allocated before the stream starts
+            srv.reserve(shape)
         rep = run_stream(srv, reqs)
         st = srv.stats()
     s = rep.summary()
@@ -355,8 +360,12 @@ def run_serving_light(rank=0, world=1, device=None, n=256, rate=30.0):
     from dda_model.replicas import max_over_ranks, shard
     from dda_model.serving import DDAServer, run_stream, synthetic_stream
 
+    from dda_model.serving import SERVE_SHAPES
+
     reqs = shard(synthetic_stream(n=n, rate=rate, seed=9), rank, world)
     with DDAServer(hbm_budget_bytes=120 * 10**9, workers=4, max_rhs=8, use_graphs=True) as srv:
+        for shape in SERVE_SHAPES:
+            srv.reserve(shape)
         rep = run_stream(srv, reqs)
     s = rep.summary()
     return {"requests": n, "arrival_rate_per_s": rate, "p50_ms": s["p50_ms"], "p99_ms": s["p99_ms"],

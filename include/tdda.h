@@ -287,6 +287,10 @@ tdda_status tdda_server_submit(tdda_server *s, const tdda_request *req, int64_t 
 /* Waits up to timeout_s (< 0: forever) for a ticket; TDDA_ERR_TIMEOUT if not
  * ready.  A ticket can be waited for once. */
 tdda_status tdda_server_wait(tdda_server *s, int64_t ticket, double timeout_s, tdda_request_result *result);
+/* Builds every worker's solve workspace for one grid (and precision) now,
+ * counted against the budget, so that the first requests of that grid do not
+ * pay for allocation.  Call before submitting requests. */
+tdda_status tdda_server_reserve(tdda_server *s, int32_t num_x, int32_t num_y, int32_t num_z, int32_t precision);
 tdda_status tdda_server_get_stats(tdda_server *s, tdda_server_stats *stats);
 /* Finishes queued work, then frees every device buffer. */
 void tdda_server_destroy(tdda_server *s);

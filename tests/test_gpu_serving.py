@@ -233,3 +233,22 @@ def test_shutdown_finishes_queued_work(sici):
     outputs = [srv._pending[t][1] for t in tickets]
     srv.close()
     assert all(np.abs(P).max() > 0 for P in outputs)
+
+
+def test_reserved_workspaces(sici):
+    """Reserving a grid allocates every worker's workspace up front (counted
+    in the budget); requests of that grid then run without allocating."""
+    from dda_model import TddaError
+
+    with _server(sici=sici, workers=2) as srv:
+        before = srv.stats()["bytes_in_use"]
+        srv.reserve((16, 16, 4))
+        after = srv.stats()["bytes_in_use"]
+        assert after > before
+        res = srv.solve(_request((16, 16, 4), seed=80))
+        assert res.info[0]["status"] == "converged"
+        assert srv.stats()["bytes_in_use"] >= after   # plus the request's tensor
+        srv.reserve((16, 16, 4))                      # already there: no change
+    with _server(sici=sici, workers=2, hbm_budget_bytes=10**7) as srv:
+        with pytest.raises(TddaError):
+            srv.reserve((64, 64, 16))

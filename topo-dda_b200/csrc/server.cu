@@ -824,6 +824,45 @@ tdda_status tdda_server_wait(tdda_server *s, int64_t ticket, double timeout_s, t
     return TDDA_OK;
 }
 
+tdda_status tdda_server_reserve(tdda_server *s, int32_t nx, int32_t ny, int32_t nz, int32_t precision) {
+    if (!s) return sbad("null argument");
+    if (nx < 1 || ny < 1 || nz < 1) return sbad("grid sizes must be positive");
+    if (precision != TDDA_PREC_MIXED && precision != TDDA_PREC_C128) return sbad("precision must be 0 or 1");
+    std::string why;
+    if (!conv_supported(nx, ny, nz, 1, 8, why) || !conv_supported(nx, ny, nz, 1, 16, why))
+        return sbad("grid not supported: " + why);
+    std::lock_guard<std::mutex> g(s->mu);
+    if (!s->queue.empty() || s->inflight > 0) return sbad("reserve before submitting requests");
+    const Shape sh{nx, ny, nz};
+    for (auto &w : s->workers) {
+        auto it = w->ws.find(sh);
+        const bool missing = it == w->ws.end();
+        size_t need = missing ? Workspace::bytes_for(nx, ny, nz, s->cfg.max_rhs) : 0;
+        const bool want64 = precision == TDDA_PREC_C128 && (missing || !it->second->has64);
+        if (want64) need += Workspace::bytes64_for(nx, ny, nz, s->cfg.max_rhs);
+        if (s->in_use + need > (size_t)s->cfg.hbm_budget_bytes) {
+            set_error("reserving workspaces for this grid exceeds the HBM budget");
+            return TDDA_ERR_OOM;
+        }
+        if (missing) {
+            std::unique_ptr<Workspace> ws(new Workspace());
+            tdda_status st = ws->init(nx, ny, nz, s->cfg.max_rhs);
+            if (st != TDDA_OK) return st;
+            it = w->ws.emplace(sh, std::move(ws)).first;
+        }
+        if (want64) {
+            const size_t keep = it->second->bytes;
+            tdda_status st = it->second->init64();
+            it->second->bytes = keep + Workspace::bytes64_for(nx, ny, nz, s->cfg.max_rhs);
+            if (st != TDDA_OK) return st;
+        }
+        s->in_use += need;
+        s->stats.peak_bytes = std::max<int64_t>(s->stats.peak_bytes, (int64_t)s->in_use);
+    }
+    s->stats.bytes_in_use = (int64_t)s->in_use;
+    return TDDA_OK;
+}
+
 tdda_status tdda_server_get_stats(tdda_server *s, tdda_server_stats *out) {
     if (!s || !out) return sbad("null argument");
     std::lock_guard<std::mutex> g(s->mu);

@@ -184,6 +184,8 @@ SIGNATURES = {
     "tdda_server_submit": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_int64)]),
     "tdda_server_wait": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_double,
                                         ctypes.POINTER(RequestResult)]),
+    "tdda_server_reserve": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                           ctypes.c_int32]),
     "tdda_server_get_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ServerStats)]),
     "tdda_server_destroy": (None, [ctypes.c_void_p]),
 }

@@ -141,6 +141,12 @@ class DDAServer:
     def solve(self, req: Request) -> Result:
         return self.wait(self.submit(req))
 
+    def reserve(self, shape, precision="mixed"):
+        """Allocate every worker's workspace for this grid now (before any
+        submit), so that the first requests of the grid do not wait for it."""
+        nx, ny, nz = (int(v) for v in shape)
+        _lib.check(self._lib.tdda_server_reserve(self._h, nx, ny, nz, PREC[precision]))
+
     def stats(self) -> dict:
         s = _lib.ServerStats()
         _lib.check(self._lib.tdda_server_get_stats(self._h, ctypes.byref(s)))
