@@ -177,6 +177,14 @@ tdda_status tdda_patch_gradient(tdda_model *m, int max_iter, double tol, double 
  * 1 complex64 (mixed-precision models only). */
 tdda_status tdda_profile_matvec(tdda_model *m, int precision, int nrhs, int iters, double *ms_matvec,
                                 double *ms_pass);
+/* No reference counterpart (measurement support): the damped periodic lattice
+ * sums -- the interaction tensor's entries before its FFT, as
+ * AProductCore::A_dic_generator forms them (src/AProductCore.cpp:335-349) --
+ * at the integer offsets lo + (i, j, k), i < nb[0], j < nb[1], k < nb[2],
+ * written to the device array out_dev: complex128 [nb0][nb1][nb2][6] (xx, xy,
+ * xz, yy, yz, zz).  At most 2^28 offsets. */
+tdda_status tdda_lattice_offsets_device(tdda_model *m, const int32_t *lo, const int32_t *nb, void *out_dev,
+                                        void *stream);
 /* Kernels launched by this library since load (all models). */
 long long tdda_kernel_launches(void);
 /* Solve precision of later solves: TDDA_PREC_C128, or TDDA_PREC_MIXED when

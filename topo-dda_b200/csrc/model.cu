@@ -1025,6 +1025,18 @@ tdda_status tdda_get_parameters(const tdda_model *m, double *out, int64_t n) {
     return TDDA_OK;
 }
 
+tdda_status tdda_lattice_offsets_device(tdda_model *m, const int32_t *lo, const int32_t *nb, void *out_dev,
+                                        void *stream) {
+    if (!m || !lo || !nb || !out_dev) return bad("null argument");
+    if (nb[0] < 1 || nb[1] < 1 || nb[2] < 1) return bad("box extents must be positive");
+    if ((long long)nb[0] * nb[1] * nb[2] > (1LL << 28)) return bad("at most 2^28 offsets");
+    cudaStream_t user = (cudaStream_t)stream;
+    TDDA_CUDA_TRY(cudaStreamSynchronize(user));
+    TRY(build_offset_tensor(m->lat, m->si_h.data(), m->ci_h.data(), (long)m->si_h.size(), lo[0], lo[1], lo[2], nb[0],
+                            nb[1], nb[2], reinterpret_cast<double2 *>(out_dev), m->stream));
+    return TDDA_OK;
+}
+
 tdda_status tdda_get_parameter_map(const tdda_model *m, int32_t *map, int64_t n) {
     if (!m || !map) return bad("null argument");
     if (n != m->N) return bad("map buffer must hold num_total entries");

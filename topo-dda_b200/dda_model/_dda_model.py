@@ -147,6 +147,13 @@ class DDAModel:
         _lib.check(self._lib.tdda_get_parameters(self._handle, _dp(g), g.size))
         return g
 
+    def lattice_offsets_device(self, lo, nb, out_ptr, stream=None):
+        """Lattice sums at the offsets lo + [0, nb) into the device array out_ptr
+        (complex128 [nb0][nb1][nb2][6]); measurement support."""
+        lo_a = (ctypes.c_int32 * 3)(*[int(v) for v in lo])
+        nb_a = (ctypes.c_int32 * 3)(*[int(v) for v in nb])
+        _lib.check(self._lib.tdda_lattice_offsets_device(self._handle, lo_a, nb_a, out_ptr, stream))
+
     def parameterMap(self):
         """Free parameter of every dipole (src/DDAModel.cpp:163-247), int32[N]."""
         out = np.zeros(self.N, dtype=np.int32)

@@ -170,6 +170,7 @@ SIGNATURES = {
     "tdda_profile_matvec": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                            _dp, _dp]),
     "tdda_kernel_launches": (ctypes.c_longlong, []),
+    "tdda_lattice_offsets_device": (ctypes.c_int, [ctypes.c_void_p, _ip, _ip, ctypes.c_void_p, ctypes.c_void_p]),
     "tdda_set_precision": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "tdda_set_preconditioner": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "tdda_set_observation_points": (ctypes.c_int, [ctypes.c_void_p, _ip, ctypes.c_int64]),
