@@ -246,8 +246,9 @@ class CpuSample:
 
 # BiCGSTAB iterations the reference's algorithm (unscaled complex128, stopping on
 # the recursive residual) takes to reach 1e-8 on the benchmark workload, as the
-# GPU arm measures it (reference_algorithm_gpu.iterations of its line)
-ITERS_PER_SOLVE = 6448
+# GPU arm measures it (reference_algorithm_gpu.iterations of its line: 6224 to
+# 6448 across runs, the count moving with round-off)
+ITERS_PER_SOLVE = 6300
 
 
 def run_reference(args):

@@ -73,7 +73,6 @@ struct Tensor {
     int users = 0;
     bool ready = false;
     bool failed = false;
-    unsigned long long last_use = 0;
 };
 
 size_t tensor_bytes(int nx, int ny, int nz) {
