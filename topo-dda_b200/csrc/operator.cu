@@ -112,6 +112,7 @@ __device__ __forceinline__ bool dfinite(double2 a) { return isfinite(a.x) && isf
 template <typename C, class Pro>
 __global__ void __launch_bounds__(NT) k_fwd_zy(ConvGeom g, C *__restrict__ T, const C *__restrict__ tw,
                                                Pro pro) {
+    pdl_wait();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *A = reinterpret_cast<C *>(smem_raw);
     C *B = A + (size_t)g.ny * g.pA;
@@ -195,6 +196,7 @@ template <typename C>
 __global__ void __launch_bounds__(NT) k_xconv(ConvGeom g, C *__restrict__ T, const C *__restrict__ ahat,
                                               const C *const *__restrict__ tab, const C *__restrict__ tw, int nrhs,
                                               const SolverState *__restrict__ st) {
+    pdl_wait();
     using R = typename RealOf<C>::type;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *Cb = reinterpret_cast<C *>(smem_raw);
@@ -262,6 +264,7 @@ template <typename C, int L>
 __global__ void __launch_bounds__(NT2) k_xconv_fast(ConvGeom g, C *__restrict__ T, const C *__restrict__ ahat,
                                                     const C *const *__restrict__ tab, const C *__restrict__ tw,
                                                     int nrhs, const SolverState *__restrict__ st) {
+    pdl_wait();
     using R = typename RealOf<C>::type;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     if (st != nullptr) {
@@ -322,12 +325,12 @@ static bool launch_xconv_fast(const ConvGeom &g, C *T, const C *ahat, const C *c
                               const SolverState *st, cudaStream_t s) {
     dim3 grid(g.Ly, g.Lz / g.CKx2, 1);
     switch (g.Lx) {
-        case 256: k_xconv_fast<C, 256><<<grid, NT2, g.smem_x2, s>>>(g, T, ahat, tab, tw, nrhs, st); return true;
-        case 128: k_xconv_fast<C, 128><<<grid, NT2, g.smem_x2, s>>>(g, T, ahat, tab, tw, nrhs, st); return true;
-        case 64: k_xconv_fast<C, 64><<<grid, NT2, g.smem_x2, s>>>(g, T, ahat, tab, tw, nrhs, st); return true;
-        case 32: k_xconv_fast<C, 32><<<grid, NT2, g.smem_x2, s>>>(g, T, ahat, tab, tw, nrhs, st); return true;
-        case 192: k_xconv_fast<C, 192><<<grid, NT2, g.smem_x2, s>>>(g, T, ahat, tab, tw, nrhs, st); return true;
-        case 96: k_xconv_fast<C, 96><<<grid, NT2, g.smem_x2, s>>>(g, T, ahat, tab, tw, nrhs, st); return true;
+        case 256: launch_dep((k_xconv_fast<C, 256>), grid, dim3(NT2), g.smem_x2, s, g, T, ahat, tab, tw, nrhs, st); return true;
+        case 128: launch_dep((k_xconv_fast<C, 128>), grid, dim3(NT2), g.smem_x2, s, g, T, ahat, tab, tw, nrhs, st); return true;
+        case 64: launch_dep((k_xconv_fast<C, 64>), grid, dim3(NT2), g.smem_x2, s, g, T, ahat, tab, tw, nrhs, st); return true;
+        case 32: launch_dep((k_xconv_fast<C, 32>), grid, dim3(NT2), g.smem_x2, s, g, T, ahat, tab, tw, nrhs, st); return true;
+        case 192: launch_dep((k_xconv_fast<C, 192>), grid, dim3(NT2), g.smem_x2, s, g, T, ahat, tab, tw, nrhs, st); return true;
+        case 96: launch_dep((k_xconv_fast<C, 96>), grid, dim3(NT2), g.smem_x2, s, g, T, ahat, tab, tw, nrhs, st); return true;
         default: return false;
     }
 }
@@ -351,6 +354,7 @@ template <typename C, int L>
 __global__ void __launch_bounds__(NTR, sizeof(C) == 8 ? 3 : 1) k_xconv_reg(ConvGeom g, C *__restrict__ T, const C *__restrict__ ahat,
                                                    const C *const *__restrict__ tab, const C *__restrict__ tw,
                                                    int nrhs, const SolverState *__restrict__ st) {
+    pdl_wait();
     using R = typename RealOf<C>::type;
     constexpr int R2 = 8, R1 = L / R2, H1 = R1 / 2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -467,11 +471,11 @@ static bool launch_xconv_reg(const ConvGeom &g, C *T, const C *ahat, const C *co
     if (!g.reg_x) return false;
     dim3 grid(g.Ly, g.Lz / g.CKr, 1);
     switch (g.Lx) {
-        case 256: k_xconv_reg<C, 256><<<grid, NTR, g.smem_r, s>>>(g, T, ahat, tab, tw, nrhs, st); return true;
-        case 192: k_xconv_reg<C, 192><<<grid, NTR, g.smem_r, s>>>(g, T, ahat, tab, tw, nrhs, st); return true;
-        case 128: k_xconv_reg<C, 128><<<grid, NTR, g.smem_r, s>>>(g, T, ahat, tab, tw, nrhs, st); return true;
-        case 96: k_xconv_reg<C, 96><<<grid, NTR, g.smem_r, s>>>(g, T, ahat, tab, tw, nrhs, st); return true;
-        case 64: k_xconv_reg<C, 64><<<grid, NTR, g.smem_r, s>>>(g, T, ahat, tab, tw, nrhs, st); return true;
+        case 256: launch_dep((k_xconv_reg<C, 256>), grid, dim3(NTR), g.smem_r, s, g, T, ahat, tab, tw, nrhs, st); return true;
+        case 192: launch_dep((k_xconv_reg<C, 192>), grid, dim3(NTR), g.smem_r, s, g, T, ahat, tab, tw, nrhs, st); return true;
+        case 128: launch_dep((k_xconv_reg<C, 128>), grid, dim3(NTR), g.smem_r, s, g, T, ahat, tab, tw, nrhs, st); return true;
+        case 96: launch_dep((k_xconv_reg<C, 96>), grid, dim3(NTR), g.smem_r, s, g, T, ahat, tab, tw, nrhs, st); return true;
+        case 64: launch_dep((k_xconv_reg<C, 64>), grid, dim3(NTR), g.smem_r, s, g, T, ahat, tab, tw, nrhs, st); return true;
         default: return false;
     }
 }
@@ -490,6 +494,7 @@ constexpr int kSmemFast = 224 * 1024;  // dynamic SMEM opt-in of the slab kernel
 template <typename C, int LZ, int LY, class Pro>
 __global__ void __launch_bounds__(NT3, 1) k_fwd_zy_fast(ConvGeom g, C *__restrict__ T, const C *__restrict__ tw,
                                                         Pro pro) {
+    pdl_wait();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *S = reinterpret_cast<C *>(smem_raw);
     constexpr int pS = LZ + 1;
@@ -512,6 +517,7 @@ __global__ void __launch_bounds__(NT3, 1) k_fwd_zy_fast(ConvGeom g, C *__restric
 template <typename C, int LZ, int LY, class Epi>
 __global__ void __launch_bounds__(NT3, 1) k_inv_yz_fast(ConvGeom g, const C *__restrict__ T,
                                                         const C *__restrict__ tw, Epi epi) {
+    pdl_wait();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *S = reinterpret_cast<C *>(smem_raw);
     constexpr int pS = LZ + 1;
@@ -568,7 +574,7 @@ static bool launch_fwd_fast(const ConvGeom &g, dim3 grid, C *T, const C *tw, con
     } else {
 #define TDDA_FWD_CASE(a, b)                                                                  \
     if (g.Lz == a && g.Ly == b) {                                                            \
-        k_fwd_zy_fast<C, a, b, Pro><<<grid, NT3, g.smem_yz2, s>>>(g, T, tw, pro);           \
+        launch_dep((k_fwd_zy_fast<C, a, b, Pro>), grid, dim3(NT3), g.smem_yz2, s, g, T, tw, pro);           \
         return true;                                                                         \
     }
         TDDA_YZ_PAIRS(TDDA_FWD_CASE)
@@ -584,7 +590,7 @@ static bool launch_inv_fast(const ConvGeom &g, dim3 grid, const C *T, const C *t
     } else {
 #define TDDA_INV_CASE(a, b)                                                                  \
     if (g.Lz == a && g.Ly == b) {                                                            \
-        k_inv_yz_fast<C, a, b, Epi><<<grid, NT3, g.smem_yz2, s>>>(g, T, tw, epi);           \
+        launch_dep((k_inv_yz_fast<C, a, b, Epi>), grid, dim3(NT3), g.smem_yz2, s, g, T, tw, epi);           \
         return true;                                                                         \
     }
         TDDA_YZ_PAIRS(TDDA_INV_CASE)
@@ -600,6 +606,7 @@ namespace tdda {
 template <typename C, class Epi>
 __global__ void __launch_bounds__(NT) k_inv_yz(ConvGeom g, const C *__restrict__ T,
                                                const C *__restrict__ tw, Epi epi) {
+    pdl_wait();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *A = reinterpret_cast<C *>(smem_raw);
     C *B = A + (size_t)g.ny * g.pA;
@@ -964,6 +971,7 @@ __global__ void __launch_bounds__(NT) k_update(long long n, C *__restrict__ P, c
                                                C *__restrict__ r, const C *__restrict__ r0,
                                                SolverState *st, double2 *part, unsigned *counter,
                                                size_t pstride) {
+    pdl_wait();
     const int rhs = blockIdx.y;
     if (st[rhs].done) return;
     const C alpha = from_d<C>(st[rhs].alpha), zeta = from_d<C>(st[rhs].zeta);
@@ -1224,16 +1232,16 @@ static tdda_status run_conv(ConvOperator<C> &op, const ConvGeom &g, int nrhs, co
     count_launches(1);
     if (!launch_fwd_reg<C, Pro>(g, g13, op.T, op.tw, pro, s) &&
         !(g.fast_yz && launch_fwd_fast<C, Pro>(g, g13, op.T, op.tw, pro, s)))
-        k_fwd_zy<C, Pro><<<g13, NT, g.smem_yz, s>>>(g, op.T, op.tw, pro);
+        launch_dep((k_fwd_zy<C, Pro>), g13, dim3(NT), g.smem_yz, s, g, op.T, op.tw, pro);
     dim3 g2(g.Ly, g.CKx > 0 ? g.Lz / g.CKx : 1, 1);
     count_launches(1);
     if (!launch_xconv_reg<C>(g, op.T, op.ahat, op.ahat_rhs, op.tw, nrhs, st, s) &&
         !(g.fast_x && launch_xconv_fast<C>(g, op.T, op.ahat, op.ahat_rhs, op.tw, nrhs, st, s)))
-        k_xconv<C><<<g2, NT, g.smem_x, s>>>(g, op.T, op.ahat, op.ahat_rhs, op.tw, nrhs, st);
+        launch_dep(k_xconv<C>, g2, dim3(NT), g.smem_x, s, g, op.T, op.ahat, op.ahat_rhs, op.tw, nrhs, st);
     count_launches(1);
     if (!launch_inv_reg<C, Epi>(g, g13, op.T, op.tw, epi, s) &&
         !(g.fast_yz && launch_inv_fast<C, Epi>(g, g13, op.T, op.tw, epi, s)))
-        k_inv_yz<C, Epi><<<g13, NT, g.smem_yz, s>>>(g, op.T, op.tw, epi);
+        launch_dep((k_inv_yz<C, Epi>), g13, dim3(NT), g.smem_yz, s, g, op.T, op.tw, epi);
     return TDDA_OK;
 }
 
@@ -1369,7 +1377,7 @@ tdda_status bicgstab_device(ConvOperator<C> &op, Krylov<C> &kv, const C *al, con
         run_conv(op, g, nrhs, pt, et, kv.st, s);
         dim3 gu(UPD_BLOCKS, nrhs);
         count_launches(1);
-        k_update<C><<<gu, NT, 0, s>>>(n, X, kv.p, kv.t, kv.At, kv.r, kv.r0, kv.st, op.partials, op.counters, ps);
+        launch_dep(k_update<C>, gu, dim3(NT), 0, s, n, X, kv.p, kv.t, kv.At, kv.r, kv.r0, kv.st, op.partials, op.counters, ps);
     };
 
     // Optional CUDA graph of graph_steps consecutive iterations, replayed

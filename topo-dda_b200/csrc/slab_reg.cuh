@@ -43,6 +43,7 @@ __host__ inline int slab_reg_smem(int ny, int LZ, int LY, bool fwd, int esize) {
 template <typename C, int LZ, int LY, class Pro>
 __global__ void __launch_bounds__(NTS, 1) k_fwd_zy_reg(ConvGeom g, C *__restrict__ T, const C *__restrict__ tw,
                                                        Pro pro) {
+    pdl_wait();
     constexpr int R1z = LZ / 8, H1z = R1z / 2, R1y = LY / 8, H1y = R1y / 2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int x = blockIdx.x, c = blockIdx.y, rhs = blockIdx.z;
@@ -120,6 +121,7 @@ __global__ void __launch_bounds__(NTS, 1) k_fwd_zy_reg(ConvGeom g, C *__restrict
 template <typename C, int LZ, int LY, class Epi>
 __global__ void __launch_bounds__(NTS, 1) k_inv_yz_reg(ConvGeom g, const C *__restrict__ T, const C *__restrict__ tw,
                                                        Epi epi) {
+    pdl_wait();
     constexpr int R1z = LZ / 8, H1z = R1z / 2, R1y = LY / 8, H1y = R1y / 2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int x = blockIdx.x, c = blockIdx.y, rhs = blockIdx.z;
@@ -208,7 +210,7 @@ static bool launch_fwd_reg(const ConvGeom &g, dim3 grid, C *T, const C *tw, cons
         if (!g.reg_yz) return false;
 #define TDDA_FWD_REG_CASE(a, b)                                                                  \
     if (g.Lz == a && g.Ly == b) {                                                                \
-        k_fwd_zy_reg<C, a, b, Pro><<<grid, NTS, g.smem_fr, s>>>(g, T, tw, pro);                 \
+        launch_dep((k_fwd_zy_reg<C, a, b, Pro>), grid, dim3(NTS), g.smem_fr, s, g, T, tw, pro);                 \
         return true;                                                                             \
     }
         TDDA_YZ_REG_PAIRS(TDDA_FWD_REG_CASE)
@@ -225,7 +227,7 @@ static bool launch_inv_reg(const ConvGeom &g, dim3 grid, const C *T, const C *tw
         if (!g.reg_yz) return false;
 #define TDDA_INV_REG_CASE(a, b)                                                                  \
     if (g.Lz == a && g.Ly == b) {                                                                \
-        k_inv_yz_reg<C, a, b, Epi><<<grid, NTS, g.smem_ir, s>>>(g, T, tw, epi);                 \
+        launch_dep((k_inv_yz_reg<C, a, b, Epi>), grid, dim3(NTS), g.smem_ir, s, g, T, tw, epi);                 \
         return true;                                                                             \
     }
         TDDA_YZ_REG_PAIRS(TDDA_INV_REG_CASE)

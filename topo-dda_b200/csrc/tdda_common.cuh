@@ -103,6 +103,34 @@ struct ConvGeom {
     int smem_x2;        // its dynamic SMEM bytes (two ping-pong buffers)
 };
 
+// ----------------------------------------------------------------------------
+// programmatic dependent launch
+// ----------------------------------------------------------------------------
+// The operator's passes and the solver's step kernels are launched with
+// programmatic stream serialization (launch_dep): the stream's next kernel may
+// be launched before the current one has fully retired.  Every kernel
+// launched through launch_dep calls pdl_wait() before its first global-memory
+// access: it returns once the previous kernel of the stream has completed and
+// its writes are visible (at once for a kernel launched without the
+// attribute, or after a copy).
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+template <typename... KArgs, typename... Args>
+inline void launch_dep(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                       const Args &...args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kern, args...);
+}
+
 int next_fft_len(int minlen);   // smallest 2^a 3^b >= minlen
 
 // number of kernels this library has launched (all devices, all models)
