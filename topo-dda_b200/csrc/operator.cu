@@ -348,9 +348,14 @@ static bool launch_xconv_fast(const ConvGeom &g, C *T, const C *ahat, const C *c
 // Tasks run with the kz index fastest, then component / right-hand side, so a
 // half-warp touches consecutive columns of a row (or rows 8 x odd pitch apart):
 // the exchanges are free of bank conflicts.
+// With g.pair_x a CTA takes ky and its mirror Ly - ky (ky = 0 and ky = Ly / 2
+// alone): both read the same folded tensor entries (the mirror with the sign
+// of the y parity), so the tensor slice one CTA reads is half as large and
+// stays in L1 for the second member.  Columns are then (member, rhs, component,
+// kz) with kz fastest.
 constexpr int NTR = 256;
 
-template <typename C, int L>
+template <typename C, int L, bool P>
 __global__ void __launch_bounds__(NTR, sizeof(C) == 8 ? 3 : 1) k_xconv_reg(ConvGeom g, C *__restrict__ T, const C *__restrict__ ahat,
                                                    const C *const *__restrict__ tab, const C *__restrict__ tw,
                                                    int nrhs, const SolverState *__restrict__ st) {
@@ -364,19 +369,21 @@ __global__ void __launch_bounds__(NTR, sizeof(C) == 8 ? 3 : 1) k_xconv_reg(ConvG
         for (int r = 0; r < nrhs; ++r) any |= (st[r].done == 0);
         if (!any) return;
     }
-    const int CK = g.CKr, ky = blockIdx.x, kz0 = blockIdx.y * CK;
-    const int ncol = nrhs * 3 * CK, ncolP = ncol | 1;
+    const int CK = g.CKr, kyA = blockIdx.x, kz0 = blockIdx.y * CK;
+    const int nky = (P && kyA != 0 && 2 * kyA != g.Ly) ? 2 : 1;   // P: g.pair_x
+    const int nrc = nrhs * 3;                 // columns per kz and member
+    const int ncomp = nrc * nky;
+    const int ncol = ncomp * CK, ncolP = ncol | 1;
     const size_t plane = (size_t)g.Ly * g.Lz;
-    const size_t off = (size_t)ky * g.Lz + kz0;
     const int twL = g.Lmax / L, twR1 = g.Lmax / R1;
     const int t = threadIdx.x;
-    const int tasks1 = ncol * R2, tasks2 = nrhs * CK * R1;
+    const int tasks1 = ncol * R2, tasks2 = nrhs * nky * CK * R1;
     // forward, first level: the column's R1-point DFT over x = 8 n1 + n2
-    const int ncomp = nrhs * 3;
     if (t < tasks1) {
         const int kl = t % CK, rest = t / CK, rc = rest % ncomp, n2 = rest / ncomp;
         const int col = rc * CK + kl;
-        const C *src = T + (size_t)rc * g.nx * plane + off + kl;
+        const int m = P ? rc / nrc : 0, ky = m ? g.Ly - kyA : kyA;
+        const C *src = T + (size_t)(rc - m * nrc) * g.nx * plane + (size_t)ky * g.Lz + kz0 + kl;
         C a[H1], b[H1];
 #pragma unroll
         for (int n1 = 0; n1 < H1; ++n1) a[n1] = src[(size_t)(R2 * n1 + n2) * plane];
@@ -396,15 +403,22 @@ __global__ void __launch_bounds__(NTR, sizeof(C) == 8 ? 3 : 1) k_xconv_reg(ConvG
     __syncthreads();
     // second level, tensor, inverse first level
     C v[3][R2];
-    int kl2 = 0, k1 = 0, rhs = 0;
+    int kl2 = 0, k1 = 0, rm = 0, rhs = 0, m = 0;
     if (t < tasks2) {
         kl2 = t % CK;
         const int rest = t / CK;
-        rhs = rest % nrhs;
-        k1 = rest / nrhs;
+        if constexpr (P) {
+            rm = rest % (nrhs * nky);
+            k1 = rest / (nrhs * nky);
+            m = rm / nrhs;
+            rhs = rm - m * nrhs;
+        } else {
+            rm = rhs = rest % nrhs;
+            k1 = rest / nrhs;
+        }
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            const int col = (rhs * 3 + c) * CK + kl2;
+            const int col = (rm * 3 + c) * CK + kl2;
 #pragma unroll
             for (int n2 = 0; n2 < R2; ++n2) v[c][n2] = S[(k1 * R2 + n2) * ncolP + col];
         }
@@ -414,7 +428,7 @@ __global__ void __launch_bounds__(NTR, sizeof(C) == 8 ? 3 : 1) k_xconv_reg(ConvG
 #pragma unroll
         for (int c = 0; c < 3; ++c) dftR<R2, -1>(v[c]);
         int fky, sy, fkz, sz;
-        fold(ky, g.Ly, fky, sy);
+        fold(m ? g.Ly - kyA : kyA, g.Ly, fky, sy);
         fold(kz0 + kl2, g.Lz, fkz, sz);
         const C *A = (tab != nullptr) ? tab[rhs] : ahat;
 #pragma unroll
@@ -442,7 +456,7 @@ __global__ void __launch_bounds__(NTR, sizeof(C) == 8 ? 3 : 1) k_xconv_reg(ConvG
         }
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            const int col = (rhs * 3 + c) * CK + kl2;
+            const int col = (rm * 3 + c) * CK + kl2;
 #pragma unroll
             for (int n1 = 0; n1 < R2; ++n1) S[(k1 * R2 + n1) * ncolP + col] = v[c][n1];
         }
@@ -452,6 +466,7 @@ __global__ void __launch_bounds__(NTR, sizeof(C) == 8 ? 3 : 1) k_xconv_reg(ConvG
     if (t < tasks1) {
         const int kl = t % CK, rest = t / CK, rc = rest % ncomp, n1 = rest / ncomp;
         const int col = rc * CK + kl;
+        const int mm = P ? rc / nrc : 0, ky = mm ? g.Ly - kyA : kyA;
         C e[H1], o[H1];
 #pragma unroll
         for (int q = 0; q < H1; ++q) {
@@ -459,9 +474,22 @@ __global__ void __launch_bounds__(NTR, sizeof(C) == 8 ? 3 : 1) k_xconv_reg(ConvG
             o[q] = S[((2 * q + 1) * R2 + n1) * ncolP + col];
         }
         dft_half_out<H1, +1>(e, o, tw, twR1);
-        C *dst = T + (size_t)rc * g.nx * plane + off + kl;
+        C *dst = T + (size_t)(rc - mm * nrc) * g.nx * plane + (size_t)ky * g.Lz + kz0 + kl;
 #pragma unroll
         for (int n2 = 0; n2 < H1; ++n2) dst[(size_t)(n1 + R2 * n2) * plane] = e[n2];
+    }
+}
+
+template <typename C, bool P>
+static bool launch_xconv_reg_t(const ConvGeom &g, dim3 grid, C *T, const C *ahat, const C *const *tab,
+                               const C *tw, int nrhs, const SolverState *st, cudaStream_t s) {
+    switch (g.Lx) {
+        case 256: launch_dep((k_xconv_reg<C, 256, P>), grid, dim3(NTR), g.smem_r, s, g, T, ahat, tab, tw, nrhs, st); return true;
+        case 192: launch_dep((k_xconv_reg<C, 192, P>), grid, dim3(NTR), g.smem_r, s, g, T, ahat, tab, tw, nrhs, st); return true;
+        case 128: launch_dep((k_xconv_reg<C, 128, P>), grid, dim3(NTR), g.smem_r, s, g, T, ahat, tab, tw, nrhs, st); return true;
+        case 96: launch_dep((k_xconv_reg<C, 96, P>), grid, dim3(NTR), g.smem_r, s, g, T, ahat, tab, tw, nrhs, st); return true;
+        case 64: launch_dep((k_xconv_reg<C, 64, P>), grid, dim3(NTR), g.smem_r, s, g, T, ahat, tab, tw, nrhs, st); return true;
+        default: return false;
     }
 }
 
@@ -469,15 +497,11 @@ template <typename C>
 static bool launch_xconv_reg(const ConvGeom &g, C *T, const C *ahat, const C *const *tab, const C *tw, int nrhs,
                              const SolverState *st, cudaStream_t s) {
     if (!g.reg_x) return false;
-    dim3 grid(g.Ly, g.Lz / g.CKr, 1);
-    switch (g.Lx) {
-        case 256: launch_dep((k_xconv_reg<C, 256>), grid, dim3(NTR), g.smem_r, s, g, T, ahat, tab, tw, nrhs, st); return true;
-        case 192: launch_dep((k_xconv_reg<C, 192>), grid, dim3(NTR), g.smem_r, s, g, T, ahat, tab, tw, nrhs, st); return true;
-        case 128: launch_dep((k_xconv_reg<C, 128>), grid, dim3(NTR), g.smem_r, s, g, T, ahat, tab, tw, nrhs, st); return true;
-        case 96: launch_dep((k_xconv_reg<C, 96>), grid, dim3(NTR), g.smem_r, s, g, T, ahat, tab, tw, nrhs, st); return true;
-        case 64: launch_dep((k_xconv_reg<C, 64>), grid, dim3(NTR), g.smem_r, s, g, T, ahat, tab, tw, nrhs, st); return true;
-        default: return false;
+    dim3 grid(g.pair_x ? g.Ly / 2 + 1 : g.Ly, g.Lz / g.CKr, 1);
+    if constexpr (sizeof(C) == 16) {
+        if (g.pair_x) return launch_xconv_reg_t<C, true>(g, grid, T, ahat, tab, tw, nrhs, st, s);
     }
+    return launch_xconv_reg_t<C, false>(g, grid, T, ahat, tab, tw, nrhs, st, s);
 }
 
 static bool reg_x_length(int L) { return L == 256 || L == 192 || L == 128 || L == 96 || L == 64; }
@@ -1054,11 +1078,18 @@ template <typename C> static void set_smem_attrs(int yz, int x) {
     cudaFuncSetAttribute(k_xconv_fast<C, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, x);
     cudaFuncSetAttribute(k_xconv_fast<C, 192>, cudaFuncAttributeMaxDynamicSharedMemorySize, x);
     cudaFuncSetAttribute(k_xconv_fast<C, 96>, cudaFuncAttributeMaxDynamicSharedMemorySize, x);
-    cudaFuncSetAttribute(k_xconv_reg<C, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, x);
-    cudaFuncSetAttribute(k_xconv_reg<C, 192>, cudaFuncAttributeMaxDynamicSharedMemorySize, x);
-    cudaFuncSetAttribute(k_xconv_reg<C, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, x);
-    cudaFuncSetAttribute(k_xconv_reg<C, 96>, cudaFuncAttributeMaxDynamicSharedMemorySize, x);
-    cudaFuncSetAttribute(k_xconv_reg<C, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, x);
+    cudaFuncSetAttribute(k_xconv_reg<C, 256, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, x);
+    cudaFuncSetAttribute(k_xconv_reg<C, 192, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, x);
+    cudaFuncSetAttribute(k_xconv_reg<C, 128, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, x);
+    cudaFuncSetAttribute(k_xconv_reg<C, 96, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, x);
+    cudaFuncSetAttribute(k_xconv_reg<C, 64, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, x);
+    if constexpr (sizeof(C) == 16) {
+        cudaFuncSetAttribute(k_xconv_reg<C, 256, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, x);
+        cudaFuncSetAttribute(k_xconv_reg<C, 192, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, x);
+        cudaFuncSetAttribute(k_xconv_reg<C, 128, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, x);
+        cudaFuncSetAttribute(k_xconv_reg<C, 96, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, x);
+        cudaFuncSetAttribute(k_xconv_reg<C, 64, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, x);
+    }
     if constexpr (std::is_same<C, float2>::value) {
         // dynamic + static shared memory must stay within the 227 KB opt-in limit;
         // the epilogue kernels carry ~1 KB of static reduction scratch
@@ -1155,20 +1186,29 @@ static bool plan_geom(int nx, int ny, int nz, int nrhs, int esize, ConvGeom &g, 
         break;
     }
     if (g.CKx2 == 0 || g.smem_x2 > SMEM_MAX) g.fast_x = 0;
-    // register-resident pass 2: one task per thread at every step
+    // register-resident pass 2: one task per thread at every step.  In
+    // complex128 ky is paired with its mirror where a kz chunk of at least 2
+    // fits the CTA that way (B200, 128x128x32: 144.0 -> 138.6 us); in complex64
+    // the halved kz chunk and the extra registers cost more than the tensor
+    // reuse gains (67.0 -> 71.2 us), so it stays unpaired.
     g.reg_x = 0;
     g.CKr = 0;
+    g.pair_x = 0;
     if (reg_x_length(g.Lx) && 2 * nx == g.Lx) {
         const int R1 = g.Lx / 8;
-        for (int ck = g.Lz; ck >= 1; --ck) {
-            if (g.Lz % ck) continue;
-            const int ncol = nrhs * 3 * ck;
-            const long long bytes = (long long)g.Lx * (ncol | 1) * esize;
-            if (nrhs * ck * R1 > NTR || ncol * 8 > NTR || bytes > SMEM_MAX) continue;
-            g.CKr = ck;
-            g.smem_r = (int)bytes;
-            g.reg_x = 1;
-            break;
+        for (int pair = (esize == 16) ? 1 : 0; pair >= 0 && !g.reg_x; --pair) {
+            const int nky = pair ? 2 : 1;
+            for (int ck = g.Lz; ck >= (pair ? 2 : 1); --ck) {
+                if (g.Lz % ck) continue;
+                const int ncol = nky * nrhs * 3 * ck;
+                const long long bytes = (long long)g.Lx * (ncol | 1) * esize;
+                if (nky * nrhs * ck * R1 > NTR || ncol * 8 > NTR || bytes > SMEM_MAX) continue;
+                g.CKr = ck;
+                g.smem_r = (int)bytes;
+                g.reg_x = 1;
+                g.pair_x = pair;
+                break;
+            }
         }
     }
     if (g.CKx == 0 && !g.fast_x && !g.reg_x) { why = "x pencils do not fit in shared memory"; return false; }

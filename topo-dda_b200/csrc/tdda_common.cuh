@@ -86,6 +86,7 @@ struct ConvGeom {
     int YC;             // y columns per z transform call (passes 1 and 3)
     int reg_x;          // pass 2 on the register-resident two-level FFT
     int CKr;            // kz chunk of that kernel
+    int pair_x;         // 1: that kernel takes ky and Ly - ky in one CTA
     int smem_r;         // its dynamic SMEM bytes
     int reg_yz;         // passes 1 and 3 on the register two-level slab kernels
     int smem_fr, smem_ir;  // their dynamic SMEM bytes (forward, inverse)
