@@ -132,19 +132,32 @@ __global__ void __launch_bounds__(NTS, 1) k_inv_yz_reg(ConvGeom g, const C *__re
     C *X = S + LZ * p.PS;
     const int twz = g.Lmax / LZ, twy = g.Lmax / LY, twz1 = g.Lmax / R1z, twy1 = g.Lmax / R1y;
     const C *Tc = T + ((size_t)(rhs * 3 + c) * g.nx + x) * (size_t)(LY * LZ);
-    // y, inverse first level: task (kz, k1) over ky = k1 + R1y k2 from T
-    for (int t = threadIdx.x; t < LZ * R1y; t += NTS) {
-        const int kz = t % LZ, k1 = t / LZ;
-        C v[8];
+    // y, inverse first level: task (kz, k1) over ky = k1 + R1y k2 from T; a
+    // thread loads the values of two tasks before transforming either, so two
+    // tasks' loads are in flight at once
+    for (int t0 = threadIdx.x; t0 < LZ * R1y; t0 += 2 * NTS) {
+        C v[2][8];
 #pragma unroll
-        for (int k2 = 0; k2 < 8; ++k2) v[k2] = Tc[(size_t)(k1 + R1y * k2) * LZ + kz];
-        dftR<8, +1>(v);
-        if (k1 != 0) {
+        for (int u = 0; u < 2; ++u) {
+            const int t = t0 + u * NTS, kz = t % LZ, k1 = t / LZ;
+            if (t < LZ * R1y) {
 #pragma unroll
-            for (int n1 = 1; n1 < 8; ++n1) v[n1] = v[n1] * twiddle<+1>(tw, k1 * n1 * twy);
+                for (int k2 = 0; k2 < 8; ++k2) v[u][k2] = Tc[(size_t)(k1 + R1y * k2) * LZ + kz];
+            }
         }
 #pragma unroll
-        for (int n1 = 0; n1 < 8; ++n1) X[(k1 * 8 + n1) * p.PY + kz] = v[n1];
+        for (int u = 0; u < 2; ++u) {
+            const int t = t0 + u * NTS, kz = t % LZ, k1 = t / LZ;
+            if (t < LZ * R1y) {
+                dftR<8, +1>(v[u]);
+                if (k1 != 0) {
+#pragma unroll
+                    for (int n1 = 1; n1 < 8; ++n1) v[u][n1] = v[u][n1] * twiddle<+1>(tw, k1 * n1 * twy);
+                }
+#pragma unroll
+                for (int n1 = 0; n1 < 8; ++n1) X[(k1 * 8 + n1) * p.PY + kz] = v[u][n1];
+            }
+        }
     }
     __syncthreads();
     // y, inverse second level: task (kz, n1), y = n1 + 8 n2 < ny into the slab
