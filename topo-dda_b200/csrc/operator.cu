@@ -378,6 +378,31 @@ __global__ void __launch_bounds__(NTR, sizeof(C) == 8 ? 3 : 1) k_xconv_reg(ConvG
     const int twL = g.Lmax / L, twR1 = g.Lmax / R1;
     const int t = threadIdx.x;
     const int tasks1 = ncol * R2, tasks2 = nrhs * nky * CK * R1;
+    // complex64: threads without a first-level task bring the tensor entries of
+    // the multiply (one folded ky, the folded kz of the chunk, every folded kx)
+    // into L1 while the others transform (shared tensor only).  B200,
+    // 128x128x32: 67.0 -> 65.1 us per launch; complex128 (paired ky) measured
+    // 140.4 -> 142.1 us with it, so it is left out there.
+    if (sizeof(C) == 8 && t >= tasks1 && tab == nullptr) {
+        int fky, sgn, lo = g.Lz, hi = 0;
+        fold(kyA, g.Ly, fky, sgn);
+        for (int kl = 0; kl < CK; ++kl) {
+            int fz;
+            fold(kz0 + kl, g.Lz, fz, sgn);
+            lo = min(lo, fz);
+            hi = max(hi, fz);
+        }
+        const int run = (hi - lo + 1) * 6 * (int)sizeof(C);  // bytes per folded kx
+        const int lines = (run + 127) / 128 + 1;
+        const char *base = reinterpret_cast<const char *>(ahat + ((size_t)fky * g.hx * g.hz + lo) * 6);
+        for (int i = t - tasks1; i < g.hx * lines; i += NTR - tasks1) {
+            const int fkx = i / lines, l = i - fkx * lines;
+            const char *p0 = base + (size_t)fkx * g.hz * 6 * sizeof(C);
+            const char *q = reinterpret_cast<const char *>(reinterpret_cast<uintptr_t>(p0) & ~(uintptr_t)127) + 128 * l;
+            if (q < p0 + run && q >= reinterpret_cast<const char *>(ahat))
+                asm volatile("prefetch.global.L1 [%0];" ::"l"(q));
+        }
+    }
     // forward, first level: the column's R1-point DFT over x = 8 n1 + n2
     if (t < tasks1) {
         const int kl = t % CK, rest = t / CK, rc = rest % ncomp, n2 = rest / ncomp;
