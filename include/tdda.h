@@ -206,10 +206,14 @@ tdda_status tdda_set_preconditioner(tdda_model *m, int kind);
  * order; the work runs on `stream`.  The only extra memory is a fixed 32 MiB
  * scratch array in the library image (held by every GPU that loads the library
  * until exit): grids needing more (2 * 3 * nx*ny*nz * 16 B + 3 * nx*Ly*Lz * 16 B)
- * are rejected with TDDA_ERR_BAD_ARG.  The first call on a device looks up the
- * scratch's device address; make it before any stream capture begins.  Calls
- * share the scratch: calls that overlap on the GPU race and must be serialised
- * by the caller. */
+ * are rejected with TDDA_ERR_BAD_ARG.  The first call on a device (and the first
+ * after its context was recreated, e.g. by cudaDeviceReset) looks up the
+ * scratch's device address, and under lazy module loading (the CUDA default)
+ * the first call on a model may load the operator kernels of its grid, which
+ * allocates device memory: make one warm-up call per model before the
+ * allocation-free region and before any stream capture begins.  Calls share
+ * the scratch: calls that overlap on the GPU race and must be serialised by
+ * the caller. */
 tdda_status tdda_matvec_device_noalloc(tdda_model *m, const void *x_dev, void *y_dev, int with_al,
                                        void *stream);
 

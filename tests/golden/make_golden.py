@@ -12,7 +12,7 @@ test_DDAModelWrapper.py:151) and stores them compactly:
   oracle_objective / oracle_iterations  this repository's oracle on the same
                         inputs (tol 1e-5), for regression.
 
-Usage: python tests/golden/make_golden.py [REFERENCE_ROOT]
+Usage: python tests/golden/make_golden.py REFERENCE_ROOT  (a Topo-DDA checkout)
 """
 import os
 import sys
@@ -53,4 +53,6 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python make_golden.py <Topo-DDA checkout root>")
+    main(sys.argv[1])

@@ -18,10 +18,18 @@
 //
 // Host code cannot use the array's name as a device address.  The first call
 // on each device looks the address up with cudaGetSymbolAddress while that
-// device is current and caches it; make that first call before any stream
-// capture begins.  All calls share the one array: calls that overlap on the
-// GPU (different streams, or different host threads) race on it and must be
-// serialised by the caller.
+// device is current and caches it together with the unique id of the device's
+// current context; a call made in another context (the primary context was
+// destroyed by cudaDeviceReset and created again, which reloads the library's
+// module, possibly at another address) looks it up again.  Under lazy module
+// loading (the CUDA default) the first call on a model may also load the
+// operator kernels of its grid, which allocates device memory: make one
+// warm-up call per model before the allocation-free region and before any
+// stream capture begins.  All calls share the one array: calls that overlap
+// on the GPU (different streams, or different host threads) race on it and
+// must be serialised by the caller.
+#include <cuda.h>
+
 #include <algorithm>
 #include <cstdio>
 #include <mutex>
@@ -39,20 +47,64 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 namespace {
 
 std::mutex g_scratch_mu;
-void *g_scratch_addr[kMaxDevices];  // device address of g_noalloc_scratch, per device
 
+// device address of g_noalloc_scratch per device, valid in the context whose
+// id is stored beside it
+struct ScratchSlot {
+    unsigned long long ctx_id;
+    void *addr;
+};
+ScratchSlot g_scratch[kMaxDevices];
+
+typedef CUresult (*CtxGetCurrentFn)(CUcontext *);
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long *);
+CtxGetCurrentFn g_ctx_get_current = nullptr;
+CtxGetIdFn g_ctx_get_id = nullptr;
+
+// Unique id of the calling thread's current context (the runtime's primary
+// context of the current device).  Context ids are never reused within a
+// process, unlike context handles.  Called with g_scratch_mu held.
+tdda_status current_context_id(unsigned long long *id) {
+    if (g_ctx_get_current == nullptr || g_ctx_get_id == nullptr) {
+        cudaDriverEntryPointQueryResult q1, q2;
+        void *f1 = nullptr, *f2 = nullptr;
+        cudaError_t e1 = cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &q1);
+        cudaError_t e2 = cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &q2);
+        if (e1 != cudaSuccess || e2 != cudaSuccess || q1 != cudaDriverEntryPointSuccess ||
+            q2 != cudaDriverEntryPointSuccess || f1 == nullptr || f2 == nullptr) {
+            set_error("cuCtxGetCurrent / cuCtxGetId are not available from the driver");
+            return TDDA_ERR_CUDA;
+        }
+        g_ctx_get_current = reinterpret_cast<CtxGetCurrentFn>(f1);
+        g_ctx_get_id = reinterpret_cast<CtxGetIdFn>(f2);
+    }
+    CUcontext ctx = nullptr;
+    if (g_ctx_get_current(&ctx) != CUDA_SUCCESS || ctx == nullptr || g_ctx_get_id(ctx, id) != CUDA_SUCCESS) {
+        set_error("no current CUDA context");
+        return TDDA_ERR_CUDA;
+    }
+    return TDDA_OK;
+}
+
+// The device address of the scratch array on device `dev` (current), looked
+// up once per device and context.
 tdda_status scratch_address(int dev, unsigned char **out) {
     std::lock_guard<std::mutex> lock(g_scratch_mu);
-    if (g_scratch_addr[dev] == nullptr) {
+    unsigned long long ctx_id = 0;
+    tdda_status st = current_context_id(&ctx_id);
+    if (st != TDDA_OK) return st;
+    ScratchSlot &slot = g_scratch[dev];
+    if (slot.addr == nullptr || slot.ctx_id != ctx_id) {
         void *p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess || p == nullptr) {
             set_error(std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
             return TDDA_ERR_CUDA;
         }
-        g_scratch_addr[dev] = p;
+        slot.addr = p;
+        slot.ctx_id = ctx_id;
     }
-    *out = static_cast<unsigned char *>(g_scratch_addr[dev]);
+    *out = static_cast<unsigned char *>(slot.addr);
     return TDDA_OK;
 }
 
