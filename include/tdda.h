@@ -197,6 +197,20 @@ tdda_status tdda_set_precision(tdda_model *m, int precision);
  * (the default for mixed-precision models). */
 tdda_status tdda_set_preconditioner(tdda_model *m, int kind);
 
+/* Solver of later solves (no reference counterpart; the reference always runs
+ * BiCGSTAB, src/DDAModel.cpp:899-1009).  kind 0: BiCGSTAB (default; the
+ * preconditioner setting above applies).  kind 1: polynomial-preconditioned
+ * restarted GMRES inside complex128 iterative refinement, for systems on which
+ * BiCGSTAB stalls (structures that fill their periodic cell): each refinement
+ * step recomputes the true residual in complex128 and runs one GMRES cycle of
+ * `restart` steps (1..256) on the Jacobi-scaled operator times a polynomial of
+ * `degree` (1..64) in it, built from the harmonic Ritz values of the first
+ * residual's Krylov space; inner solves in complex64 for mixed-precision
+ * models.  The solve stops when ||E - A P|| / ||E|| <= tol; max_iter bounds the
+ * inner operator applications (tdda_solve_info: iterations = GMRES steps,
+ * inner_iterations = operator applications, refinements = cycles). */
+tdda_status tdda_set_solver(tdda_model *m, int kind, int degree, int restart);
+
 /* Allocation-free A.x (+ (1/alpha) o x when with_al != 0) for one vector.
  * No counterpart in the reference.  For callers that must not have device
  * memory allocated during a call -- a serving loop admitting work against a

@@ -1,0 +1,81 @@
+"""The polynomial-preconditioned GMRES solver (tdda_set_solver kind 1) vs the
+oracle: the true residual of its solution, recomputed with the oracle's
+complex128 operator, meets the tolerance, and the solution agrees with the
+oracle's dense direct solve within the conditioning of the system
+(1e3 x tol), in complex128 and in mixed precision, for periodic structures
+that fill their cell (where the solver is meant to be used), non-box
+geometries and several right-hand sides at once."""
+import numpy as np
+import pytest
+
+from cases import model_args, rel
+
+pytestmark = pytest.mark.gpu
+
+
+def _solve(kw, precision, degree, restart, tol, B, max_iter=200000):
+    import torch
+
+    from dda_model import DDAModel
+
+    m = DDAModel(**kw, precision=precision)
+    m.setSolver("pgmres", degree=degree, restart=restart)
+    nrhs = B.shape[0]
+    Bd = torch.from_numpy(B).cuda()
+    X = torch.zeros_like(Bd)
+    infos = m.solve_batch_device(Bd.data_ptr(), X.data_ptr(), nrhs, True, max_iter, tol,
+                                 torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    return X.cpu().numpy(), infos
+
+
+def _rhs(ora, nrhs, seed):
+    r = np.random.default_rng(seed)
+    B = [ora.E]
+    for _ in range(nrhs - 1):
+        B.append(r.standard_normal(3 * ora.N) + 1j * r.standard_normal(3 * ora.N))
+    return np.ascontiguousarray(np.stack(B))
+
+
+@pytest.mark.parametrize("precision", ["complex128", "mixed"])
+@pytest.mark.parametrize("shape,M,subset,nrhs", [((12, 12, 6), 20, False, 1), ((10, 8, 4), 5, True, 2),
+                                                 ((16, 16, 8), 50, False, 1)])
+def test_pgmres_matches_oracle(sici, precision, shape, M, subset, nrhs):
+    from oracle.dda_oracle import OracleModel, generate_geometry
+
+    nx, ny, nz = shape
+    geo, rho = None, None
+    if subset:
+        g = generate_geometry(nx, ny, nz).reshape(-1, 3)
+        keep = (g[:, 0] * 3 + g[:, 1] + 2 * g[:, 2]) % 5 != 0
+        geo = g[keep].ravel()
+        rho = np.random.default_rng(4).random(keep.sum())
+    kw = model_args(nx, ny, nz, sici, MAXm=M, MAXn=M, seed=9, geometry=geo, rho=rho)
+    ora = OracleModel(**kw)
+    B = _rhs(ora, nrhs, 3)
+    tol = 1e-8
+    X, infos = _solve(kw, precision, 8, 12, tol, B)
+    A = ora.dense_operator() if ora.N <= 1500 else None
+    for k in range(nrhs):
+        assert infos[k]["status"] == "converged", infos[k]
+        res = np.linalg.norm(B[k] - ora.aproduct_with_alb(X[k])) / np.linalg.norm(B[k])
+        assert res <= 1.0001 * tol, (k, res, infos[k])
+        assert abs(infos[k]["true_error"] - res) <= 1e-3 * tol, (infos[k]["true_error"], res)
+        if A is not None:
+            x = np.linalg.solve(A, B[k])
+            assert rel(X[k], x) < 1e3 * tol
+
+
+def test_pgmres_iteration_budget(sici):
+    """max_iter bounds the inner operator applications (checked between
+    cycles), and the counts in the info are consistent."""
+    from oracle.dda_oracle import OracleModel
+
+    kw = model_args(12, 12, 6, sici, MAXm=20, MAXn=20, seed=9)
+    B = _rhs(OracleModel(**kw), 1, 1)
+    X, infos = _solve(kw, "complex128", 6, 5, 1e-15, B, max_iter=40)
+    i = infos[0]
+    assert i["status"] == "max_iter", i
+    assert i["inner_iterations"] >= i["iterations"] * 6
+    # the polynomial's 6 steps, one cycle of 5 x 6, the correction's 6, then the budget check
+    assert 40 <= i["inner_iterations"] <= 40 + 6 * 5 + 6, i

@@ -1,0 +1,643 @@
+// Polynomial-preconditioned GMRES in complex128 refinement (see gmres.cuh).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "gmres.cuh"
+
+namespace tdda {
+
+// ----------------------------------------------------------------------------
+// Gram-Schmidt kernels: all sums in FP64, block partials added in block order
+// (deterministic).  Vectors of right-hand side k start at k * rstr; basis
+// vector i starts at i * vstr.
+// ----------------------------------------------------------------------------
+constexpr int kGsThreads = 256;
+constexpr int kGsBlocks = 148 * 4;
+constexpr int kGsChunk = 8;   // basis vectors per multi-dot CTA
+
+template <int NV> __device__ __forceinline__ void block_sum_v(double2 (&v)[NV], double2 *sm) {
+    // sm: NV * (kGsThreads / 32) double2
+#pragma unroll
+    for (int k = 0; k < NV; ++k)
+        for (int o = 16; o > 0; o >>= 1) {
+            v[k].x += __shfl_down_sync(0xffffffffu, v[k].x, o);
+            v[k].y += __shfl_down_sync(0xffffffffu, v[k].y, o);
+        }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) sm[k * (kGsThreads / 32) + warp] = v[k];
+    __syncthreads();
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            double2 t = sm[k * (kGsThreads / 32)];
+            for (int w = 1; w < kGsThreads / 32; ++w) {
+                t.x += sm[k * (kGsThreads / 32) + w].x;
+                t.y += sm[k * (kGsThreads / 32) + w].y;
+            }
+            v[k] = t;
+        }
+}
+
+// part[(k * nv + i) * gridDim.x + blk] = this block's share of conj(V_i[k]) . w[k]
+template <typename C>
+__global__ void __launch_bounds__(kGsThreads) k_multidot(long long n, int nv, const C *__restrict__ V, size_t vstr,
+                                                         size_t rstr, const C *__restrict__ w,
+                                                         double2 *__restrict__ part) {
+    pdl_wait();
+    __shared__ double2 sm[kGsChunk * (kGsThreads / 32)];
+    const int k = blockIdx.z, i0 = blockIdx.y * kGsChunk;
+    const int nb = min(kGsChunk, nv - i0);
+    double2 acc[kGsChunk];
+#pragma unroll
+    for (int q = 0; q < kGsChunk; ++q) acc[q] = make_double2(0.0, 0.0);
+    const C *wk = w + (size_t)k * rstr;
+    const C *Vk = V + (size_t)k * rstr + (size_t)i0 * vstr;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        const double2 wv = to_d(__ldg(wk + e));
+#pragma unroll
+        for (int q = 0; q < kGsChunk; ++q)
+            if (q < nb) {
+                const double2 d = cdot1(to_d(__ldg(Vk + (size_t)q * vstr + e)), wv);
+                acc[q].x += d.x;
+                acc[q].y += d.y;
+            }
+    }
+    block_sum_v<kGsChunk>(acc, sm);
+    if (threadIdx.x == 0)
+        for (int q = 0; q < nb; ++q) part[((size_t)k * nv + i0 + q) * gridDim.x + blockIdx.x] = acc[q];
+}
+
+// out[j] = sum over blocks (in order) of part[j * nblk + b], one warp per j;
+// with nrm != nullptr the entries are squared norms (real part): nrm[j] gets
+// the square root of the sum and inv[j] its reciprocal (0 for a zero norm).
+__global__ void k_sum_parts(int nout, int nblk, const double2 *__restrict__ part, double2 *__restrict__ out,
+                            double *__restrict__ nrm, double *__restrict__ inv) {
+    pdl_wait();
+    const int j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (j >= nout) return;
+    double2 t = make_double2(0.0, 0.0);
+    for (int b = lane; b < nblk; b += 32) {
+        t.x += part[(size_t)j * nblk + b].x;
+        t.y += part[(size_t)j * nblk + b].y;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        t.x += __shfl_down_sync(0xffffffffu, t.x, o);
+        t.y += __shfl_down_sync(0xffffffffu, t.y, o);
+    }
+    if (lane == 0) {
+        if (out != nullptr) out[j] = t;
+        if (nrm != nullptr) {
+            const double r = sqrt(fmax(t.x, 0.0));
+            nrm[j] = r;
+            inv[j] = r > 0.0 ? 1.0 / r : 0.0;
+        }
+    }
+}
+
+// w[k] -= sum_{i < nv} h[k * hstr + i] V_i[k]; with part != nullptr also the
+// block's share of ||w[k]||^2 (after the update) into part[k * gridDim.x + blk]
+template <typename C>
+__global__ void __launch_bounds__(kGsThreads) k_gs_update(long long n, int nv, const C *__restrict__ V, size_t vstr,
+                                                          size_t rstr, const double2 *__restrict__ h, int hstr,
+                                                          C *__restrict__ w, double2 *__restrict__ part) {
+    pdl_wait();
+    extern __shared__ double2 hs[];
+    __shared__ double2 sm[kGsThreads / 32];
+    const int k = blockIdx.z;
+    for (int i = threadIdx.x; i < nv; i += blockDim.x) hs[i] = h[(size_t)k * hstr + i];
+    __syncthreads();
+    C *wk = w + (size_t)k * rstr;
+    const C *Vk = V + (size_t)k * rstr;
+    double2 acc[1] = {make_double2(0.0, 0.0)};
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        double2 v = to_d(wk[e]);
+        for (int i = 0; i < nv; ++i) {
+            const double2 b = to_d(__ldg(Vk + (size_t)i * vstr + e));
+            const double2 c = hs[i];
+            v.x -= c.x * b.x - c.y * b.y;
+            v.y -= c.x * b.y + c.y * b.x;
+        }
+        const C vc = from_d<C>(v);
+        wk[e] = vc;
+        const double2 vd = to_d(vc);
+        acc[0].x += vd.x * vd.x + vd.y * vd.y;
+    }
+    if (part != nullptr) {
+        block_sum_v<1>(acc, sm);
+        if (threadIdx.x == 0) part[(size_t)k * gridDim.x + blockIdx.x] = acc[0];
+    }
+}
+
+// out[k] = s[k] * x[k]   (s: device reals, one per right-hand side)
+template <typename C>
+__global__ void __launch_bounds__(kGsThreads) k_scale_vec(long long n, size_t rstr, const double *__restrict__ s,
+                                                          const C *__restrict__ x, C *__restrict__ out) {
+    pdl_wait();
+    const int k = blockIdx.z;
+    const double f = s[k];
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        const double2 v = to_d(x[(size_t)k * rstr + e]);
+        out[(size_t)k * rstr + e] = from_d<C>(make_double2(f * v.x, f * v.y));
+    }
+}
+
+// out[k] = sum_{i < nv} y[k * ystr + i] V_i[k]
+template <typename C>
+__global__ void __launch_bounds__(kGsThreads) k_lincomb(long long n, int nv, const C *__restrict__ V, size_t vstr,
+                                                        size_t rstr, const double2 *__restrict__ y, int ystr,
+                                                        C *__restrict__ out) {
+    pdl_wait();
+    extern __shared__ double2 ys[];
+    const int k = blockIdx.z;
+    for (int i = threadIdx.x; i < nv; i += blockDim.x) ys[i] = y[(size_t)k * ystr + i];
+    __syncthreads();
+    const C *Vk = V + (size_t)k * rstr;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        double2 v = make_double2(0.0, 0.0);
+        for (int i = 0; i < nv; ++i) {
+            const double2 b = to_d(__ldg(Vk + (size_t)i * vstr + e));
+            const double2 c = ys[i];
+            v.x += c.x * b.x - c.y * b.y;
+            v.y += c.x * b.y + c.y * b.x;
+        }
+        out[(size_t)k * rstr + e] = from_d<C>(v);
+    }
+}
+
+// ----------------------------------------------------------------------------
+// workspace
+// ----------------------------------------------------------------------------
+template <typename C> size_t GmresWork<C>::bytes() const {
+    const size_t vec = sizeof(C) * (size_t)n * nrhs;
+    return vec * (restart + 3) +
+           sizeof(double2) * ((size_t)kGsBlocks * nrhs * (restart + 1) + 3 * (size_t)nrhs * (restart + 1)) +
+           sizeof(double) * 2 * nrhs;
+}
+
+template <typename C> tdda_status GmresWork<C>::init(long long n3, int nrhs_, int restart_, int degree_) {
+    release();
+    n = n3; nrhs = nrhs_; restart = restart_; degree = degree_;
+    const size_t vec = (size_t)n * nrhs;
+    TDDA_CUDA_TRY(cudaMalloc(&V, sizeof(C) * vec * (restart + 1)));
+    TDDA_CUDA_TRY(cudaMalloc(&W, sizeof(C) * vec));
+    TDDA_CUDA_TRY(cudaMalloc(&Y, sizeof(C) * vec));
+    // cells without a dipole must read as zero in every vector
+    TDDA_CUDA_TRY(cudaMemset(V, 0, sizeof(C) * vec * (restart + 1)));
+    TDDA_CUDA_TRY(cudaMemset(W, 0, sizeof(C) * vec));
+    TDDA_CUDA_TRY(cudaMemset(Y, 0, sizeof(C) * vec));
+    TDDA_CUDA_TRY(cudaMalloc(&part, sizeof(double2) * (size_t)kGsBlocks * nrhs * (restart + 1)));
+    TDDA_CUDA_TRY(cudaMalloc(&h, sizeof(double2) * 2 * (size_t)nrhs * (restart + 1)));
+    TDDA_CUDA_TRY(cudaMalloc(&coef, sizeof(double2) * (size_t)nrhs * (restart + 1)));
+    TDDA_CUDA_TRY(cudaMalloc(&nrm, sizeof(double) * 2 * nrhs));
+    TDDA_CUDA_TRY(cudaMallocHost(&h_host, sizeof(double2) * (2 * (size_t)nrhs * (restart + 1) + nrhs)));
+    return TDDA_OK;
+}
+
+template <typename C> void GmresWork<C>::release() {
+    cudaFree(V); cudaFree(W); cudaFree(Y); cudaFree(part); cudaFree(h); cudaFree(coef); cudaFree(nrm);
+    cudaFreeHost(h_host);
+    V = W = Y = nullptr;
+    part = h = coef = nullptr;
+    nrm = nullptr;
+    h_host = nullptr;
+    nrhs = 0;
+}
+
+// ----------------------------------------------------------------------------
+// host linear algebra of the polynomial
+// ----------------------------------------------------------------------------
+bool hessenberg_eigenvalues(cplx *H, int n, int ld, std::vector<cplx> &ev) {
+    auto h = [&](int i, int j) -> cplx & { return H[i + (size_t)j * ld]; };
+    ev.assign(n, cplx(0.0, 0.0));
+    int hi = n - 1, iter = 0;
+    while (hi >= 0) {
+        if (hi == 0) { ev[0] = h(0, 0); break; }
+        int lo = hi;
+        while (lo > 0) {
+            double s = std::abs(h(lo - 1, lo - 1)) + std::abs(h(lo, lo));
+            if (s == 0.0) s = 1.0;
+            if (std::abs(h(lo, lo - 1)) <= 1e-15 * s) { h(lo, lo - 1) = 0.0; break; }
+            --lo;
+        }
+        if (lo == hi) { ev[hi] = h(hi, hi); --hi; iter = 0; continue; }
+        if (++iter > 60 * (hi - lo + 1)) return false;
+        // Wilkinson shift: the eigenvalue of the trailing 2x2 block nearer h(hi, hi)
+        const cplx a = h(hi - 1, hi - 1), b = h(hi - 1, hi), c = h(hi, hi - 1), d = h(hi, hi);
+        const cplx tr = a + d, det = a * d - b * c;
+        const cplx disc = std::sqrt(tr * tr / 4.0 - det);
+        const cplx l1 = tr / 2.0 + disc, l2 = tr / 2.0 - disc;
+        cplx mu = (std::abs(l1 - d) < std::abs(l2 - d)) ? l1 : l2;
+        if (iter % 11 == 10) mu = d + cplx(std::abs(c), 0.0);  // exceptional shift
+        // H - mu I = Q R by Givens rotations, then H <- R Q + mu I on the active block
+        for (int k = lo; k <= hi; ++k) h(k, k) -= mu;
+        std::vector<cplx> cs(hi - lo), sn(hi - lo);
+        for (int k = lo; k < hi; ++k) {
+            const cplx x = h(k, k), y = h(k + 1, k);
+            const double r = std::sqrt(std::norm(x) + std::norm(y));
+            const cplx cc = r == 0.0 ? cplx(1.0) : x / r, ss = r == 0.0 ? cplx(0.0) : y / r;
+            cs[k - lo] = cc;
+            sn[k - lo] = ss;
+            for (int j = k; j < n; ++j) {
+                const cplx u = h(k, j), v = h(k + 1, j);
+                h(k, j) = std::conj(cc) * u + std::conj(ss) * v;
+                h(k + 1, j) = -ss * u + cc * v;
+            }
+        }
+        for (int k = lo; k < hi; ++k) {
+            const cplx cc = cs[k - lo], ss = sn[k - lo];
+            for (int i = 0; i <= std::min(k + 2, hi); ++i) {
+                const cplx u = h(i, k), v = h(i, k + 1);
+                h(i, k) = u * cc + v * ss;
+                h(i, k + 1) = -u * std::conj(ss) + v * std::conj(cc);
+            }
+        }
+        for (int k = lo; k <= hi; ++k) h(k, k) += mu;
+    }
+    return true;
+}
+
+// Dense n x n solve by Gaussian elimination with partial pivoting
+// (column-major, ld; A and b destroyed).
+static bool dense_solve(cplx *A, int n, int ld, cplx *b) {
+    auto a = [&](int i, int j) -> cplx & { return A[i + (size_t)j * ld]; };
+    for (int k = 0; k < n; ++k) {
+        int p = k;
+        for (int i = k + 1; i < n; ++i)
+            if (std::abs(a(i, k)) > std::abs(a(p, k))) p = i;
+        if (a(p, k) == cplx(0.0)) return false;
+        if (p != k) {
+            for (int j = 0; j < n; ++j) std::swap(a(k, j), a(p, j));
+            std::swap(b[k], b[p]);
+        }
+        for (int i = k + 1; i < n; ++i) {
+            const cplx f = a(i, k) / a(k, k);
+            if (f == cplx(0.0)) continue;
+            for (int j = k; j < n; ++j) a(i, j) -= f * a(k, j);
+            b[i] -= f * b[k];
+        }
+    }
+    for (int i = n - 1; i >= 0; --i) {
+        cplx s = b[i];
+        for (int j = i + 1; j < n; ++j) s -= a(i, j) * b[j];
+        b[i] = s / a(i, i);
+    }
+    return true;
+}
+
+bool harmonic_ritz(const cplx *Hbar, int d, int ld, std::vector<cplx> &theta) {
+    // eigenvalues of H_d + |h_{d+1,d}|^2 f e_d^T with H_d^H f = e_d (still
+    // upper Hessenberg: only the last column changes)
+    std::vector<cplx> Ht((size_t)d * d), f(d, cplx(0.0)), M((size_t)d * d);
+    for (int i = 0; i < d; ++i)
+        for (int j = 0; j < d; ++j) Ht[i + (size_t)j * d] = std::conj(Hbar[j + (size_t)i * ld]);
+    f[d - 1] = 1.0;
+    if (!dense_solve(Ht.data(), d, d, f.data())) return false;
+    const double h2 = std::norm(Hbar[d + (size_t)(d - 1) * ld]);
+    for (int i = 0; i < d; ++i)
+        for (int j = 0; j < d; ++j) M[i + (size_t)j * d] = (i <= j + 1) ? Hbar[i + (size_t)j * ld] : cplx(0.0);
+    for (int i = 0; i < d; ++i) M[i + (size_t)(d - 1) * d] += h2 * f[i];
+    return hessenberg_eigenvalues(M.data(), d, d, theta);
+}
+
+void leja_order(std::vector<cplx> &th) {
+    const int d = (int)th.size();
+    if (d == 0) return;
+    std::vector<cplx> out;
+    std::vector<char> used(d, 0);
+    int k0 = 0;
+    for (int i = 1; i < d; ++i)
+        if (std::abs(th[i]) > std::abs(th[k0])) k0 = i;
+    out.push_back(th[k0]);
+    used[k0] = 1;
+    std::vector<double> lp(d, 0.0);  // log of the product of distances to the roots taken
+    for (int step = 1; step < d; ++step) {
+        int best = -1;
+        for (int i = 0; i < d; ++i) {
+            if (used[i]) continue;
+            lp[i] += std::log(std::abs(th[i] - out.back()) + 1e-300);
+            if (best < 0 || lp[i] > lp[best]) best = i;
+        }
+        out.push_back(th[best]);
+        used[best] = 1;
+    }
+    // a root whose other factors multiply to more than 1e4 at it gets one
+    // extra copy per 14 decades beyond (the product form stays stable)
+    std::vector<cplx> extra;
+    for (int i = 0; i < d; ++i) {
+        double pof = 0.0;
+        for (int j = 0; j < d; ++j)
+            if (j != i) pof += std::log10(std::abs(1.0 - out[i] / out[j]));
+        if (pof > 4.0) {
+            const int copies = (int)std::ceil((pof - 4.0) / 14.0);
+            for (int c = 0; c < copies; ++c) extra.push_back(out[i]);
+        }
+    }
+    out.insert(out.end(), extra.begin(), extra.end());
+    th.swap(out);
+}
+
+// ----------------------------------------------------------------------------
+// the solver
+// ----------------------------------------------------------------------------
+namespace {
+
+unsigned gs_blocks(long long n) {
+    return (unsigned)std::max<long long>(1, std::min<long long>((n + kGsThreads - 1) / kGsThreads, kGsBlocks));
+}
+
+template <typename C> C *basis(GmresWork<C> &gw, int i) { return gw.V + (size_t)i * gw.n * gw.nrhs; }
+
+// h[k * nv + i] = V_i[k]^H w[k], i < nv (device)
+template <typename C> void multidot(GmresWork<C> &gw, int nv, const C *w, double2 *h, cudaStream_t s) {
+    const size_t rstr = gw.n, vstr = (size_t)gw.n * gw.nrhs;
+    const unsigned nb = gs_blocks(gw.n);
+    count_launches(2);
+    launch_dep(k_multidot<C>, dim3(nb, (nv + kGsChunk - 1) / kGsChunk, gw.nrhs), dim3(kGsThreads), 0, s, gw.n, nv,
+               (const C *)gw.V, vstr, rstr, w, gw.part);
+    const int nout = gw.nrhs * nv;
+    launch_dep(k_sum_parts, dim3((nout + 7) / 8), dim3(256), 0, s, nout, (int)nb, (const double2 *)gw.part, h,
+               (double *)nullptr, (double *)nullptr);
+}
+
+// w[k] -= V[0..nv)[k] h[k]; with norms: nrm[k] = ||w[k]||, nrm[nrhs + k] = 1 / nrm[k]
+template <typename C>
+void gs_update(GmresWork<C> &gw, int nv, const double2 *h, int hstr, C *w, bool norms, cudaStream_t s) {
+    const size_t rstr = gw.n, vstr = (size_t)gw.n * gw.nrhs;
+    const unsigned nb = gs_blocks(gw.n);
+    count_launches(1);
+    launch_dep(k_gs_update<C>, dim3(nb, 1, gw.nrhs), dim3(kGsThreads), sizeof(double2) * std::max(nv, 1), s, gw.n,
+               nv, (const C *)gw.V, vstr, rstr, h, hstr, w, norms ? gw.part : (double2 *)nullptr);
+    if (norms) {
+        count_launches(1);
+        launch_dep(k_sum_parts, dim3((gw.nrhs + 7) / 8), dim3(256), 0, s, gw.nrhs, (int)nb, (const double2 *)gw.part,
+                   (double2 *)nullptr, gw.nrm, gw.nrm + gw.nrhs);
+    }
+}
+
+template <typename C> void scale_vec(GmresWork<C> &gw, const double *f, const C *x, C *out, cudaStream_t s) {
+    count_launches(1);
+    launch_dep(k_scale_vec<C>, dim3(gs_blocks(gw.n), 1, gw.nrhs), dim3(kGsThreads), 0, s, gw.n, (size_t)gw.n, f, x,
+               out);
+}
+
+// One Arnoldi step on operator `op_fn` (v_j -> V[j+1]) with classical
+// Gram-Schmidt and one reorthogonalisation; the Hessenberg column of every
+// right-hand side lands in Hcol[k][0..j+1] (host, after the copy).
+template <typename C, class OpFn>
+tdda_status arnoldi_step(GmresWork<C> &gw, int j, OpFn op_fn, std::vector<std::vector<cplx>> &Hcol, cudaStream_t s) {
+    const int nv = j + 1, nr = gw.nrhs, hs = gw.restart + 1;
+    C *w = basis(gw, j + 1);
+    tdda_status st = op_fn(basis(gw, j), w);
+    if (st != TDDA_OK) return st;
+    double2 *h1 = gw.h, *h2 = gw.h + (size_t)nr * hs;
+    multidot(gw, nv, w, h1, s);
+    gs_update(gw, nv, h1, nv, w, false, s);
+    multidot(gw, nv, w, h2, s);
+    gs_update(gw, nv, h2, nv, w, true, s);
+    scale_vec(gw, gw.nrm + nr, w, w, s);
+    double2 *hh = gw.h_host;
+    TDDA_CUDA_TRY(cudaMemcpyAsync(hh, gw.h, sizeof(double2) * 2 * (size_t)nr * hs, cudaMemcpyDeviceToHost, s));
+    TDDA_CUDA_TRY(cudaMemcpyAsync(hh + 2 * (size_t)nr * hs, gw.nrm, sizeof(double) * nr, cudaMemcpyDeviceToHost, s));
+    TDDA_CUDA_TRY(cudaStreamSynchronize(s));
+    TDDA_CUDA_TRY(cudaGetLastError());
+    const double *nrm = reinterpret_cast<const double *>(hh + 2 * (size_t)nr * hs);
+    for (int k = 0; k < nr; ++k) {
+        Hcol[k].assign(nv + 1, cplx(0.0));
+        for (int i = 0; i < nv; ++i) {
+            const double2 a = hh[(size_t)k * nv + i], b = hh[(size_t)nr * hs + (size_t)k * nv + i];
+            Hcol[k][i] = cplx(a.x + b.x, a.y + b.y);
+        }
+        Hcol[k][nv] = cplx(nrm[k], 0.0);
+    }
+    return TDDA_OK;
+}
+
+// Givens QR of one right-hand side's Hessenberg matrix, column by column.
+struct Givens {
+    int m = 0;
+    std::vector<cplx> R;   // (m + 1) x m column-major, rotated
+    std::vector<cplx> c, s, g;
+    void reset(int m_, double beta) {
+        m = m_;
+        R.assign((size_t)(m + 1) * m, cplx(0.0));
+        c.assign(m, cplx(0.0));
+        s.assign(m, cplx(0.0));
+        g.assign(m + 1, cplx(0.0));
+        g[0] = beta;
+    }
+    // adds column j (entries 0..j+1); returns |residual estimate|
+    double add(int j, const std::vector<cplx> &col) {
+        cplx *Rj = &R[(size_t)j * (m + 1)];
+        for (int i = 0; i <= j + 1; ++i) Rj[i] = col[i];
+        for (int i = 0; i < j; ++i) {
+            const cplx t = c[i] * Rj[i] + s[i] * Rj[i + 1];
+            Rj[i + 1] = -std::conj(s[i]) * Rj[i] + std::conj(c[i]) * Rj[i + 1];
+            Rj[i] = t;
+        }
+        const cplx a = Rj[j], b = Rj[j + 1];
+        const double den = std::sqrt(std::norm(a) + std::norm(b));
+        if (den == 0.0) {
+            c[j] = 1.0;
+            s[j] = 0.0;
+        } else {
+            c[j] = std::conj(a) / den;
+            s[j] = std::conj(b) / den;
+        }
+        Rj[j] = den;
+        Rj[j + 1] = 0.0;
+        g[j + 1] = -std::conj(s[j]) * g[j];
+        g[j] = c[j] * g[j];
+        return std::abs(g[j + 1]);
+    }
+    // least-squares solution of the first k columns
+    void solve(int k, std::vector<cplx> &y) const {
+        y.assign(k, cplx(0.0));
+        for (int i = k - 1; i >= 0; --i) {
+            cplx t = g[i];
+            for (int l = i + 1; l < k; ++l) t -= R[(size_t)l * (m + 1) + i] * y[l];
+            const cplx d = R[(size_t)i * (m + 1) + i];
+            y[i] = d == cplx(0.0) ? cplx(0.0) : t / d;
+        }
+    }
+};
+
+}  // namespace
+
+template <typename C>
+tdda_status pgmres_solve(const RefineWork<C> &w, GmresWork<C> &gw, const double2 *B, double2 *X, int nrhs,
+                         bool x0_zero, int max_iter, double tol, const GmresOptions &o, tdda_solve_info *info) {
+    const long long n = 3 * w.nbox;
+    cudaStream_t s = w.s;
+    if (gw.nrhs != nrhs || gw.n != n || gw.restart != o.restart || gw.degree != o.degree) {
+        set_error("GMRES workspace does not match the solve");
+        return TDDA_ERR_STATE;
+    }
+    if (x0_zero) TDDA_CUDA_TRY(cudaMemsetAsync(X, 0, sizeof(double2) * n * nrhs, s));
+    const int m = o.restart, d = o.degree;
+    std::vector<int> done(nrhs, 0), cycles(nrhs, 0), steps(nrhs, 0), status(nrhs, TDDA_SOLVE_RUNNING), slow(nrhs, 0);
+    std::vector<long long> mv(nrhs, 0);
+    std::vector<double> err(nrhs, 0.0), prev(nrhs, 1e300), beta(nrhs, 0.0);
+    std::vector<cplx> roots;
+    std::vector<std::vector<cplx>> Hcol(nrhs);
+    std::vector<Givens> qr(nrhs);
+    double *h = w.h_part;
+    // the inner operator, and the inner operator times the polynomial
+    auto op_plain = [&](const C *x, C *y) { return apply_scaled<C>(*w.op, w.sc, w.al, x, y, nrhs, w.dstride, s); };
+    auto op_poly = [&](const C *v, C *out) -> tdda_status {
+        // out = v - prod(1 - Ah / theta_i) v  =  Ah p(Ah) v
+        const int nr = (int)roots.size();
+        for (int i = 0; i < nr; ++i) {
+            const cplx c = 1.0 / roots[i];
+            const C *rin = i == 0 ? v : gw.W;
+            const bool last = i == nr - 1;
+            tdda_status st = poly_factor<C>(*w.op, w.sc, w.al, rin, gw.W, nullptr, false, last ? v : nullptr,
+                                            last ? out : nullptr, make_double2(c.real(), c.imag()), nrhs, w.dstride, s);
+            if (st != TDDA_OK) return st;
+        }
+        return TDDA_OK;
+    };
+    const int max_cycles = 100000;
+    for (int cycle = 0; cycle <= max_cycles; ++cycle) {
+        tdda_status st = residual_c128(*w.op64, w.al64, B, X, w.Rm, w.st_res, nrhs, s, w.dstride);
+        if (st != TDDA_OK) return st;
+        TDDA_CUDA_TRY(cudaMemcpyAsync(w.st_res_host, w.st_res, sizeof(SolverState) * nrhs, cudaMemcpyDeviceToHost, s));
+        TDDA_CUDA_TRY(cudaStreamSynchronize(s));
+        bool all = true;
+        for (int k = 0; k < nrhs; ++k) {
+            if (done[k]) continue;
+            const SolverState &S = w.st_res_host[k];
+            err[k] = S.err;
+            if (S.enorm == 0.0) {
+                TDDA_CUDA_TRY(cudaMemsetAsync(X + (size_t)k * n, 0, sizeof(double2) * n, s));
+                done[k] = 1; status[k] = TDDA_SOLVE_ZERO_RHS; err[k] = 0.0;
+            } else if (S.err <= tol) {
+                done[k] = 1; status[k] = TDDA_SOLVE_CONVERGED;
+            } else if (!std::isfinite(S.err)) {
+                done[k] = 1; status[k] = TDDA_SOLVE_NONFINITE;
+            } else if (mv[k] >= max_iter || cycle == max_cycles) {
+                done[k] = 1; status[k] = TDDA_SOLVE_MAXITER;
+            } else {
+                // six cycles in a row that each gain less than 1%: stagnated
+                slow[k] = (S.err > 0.99 * prev[k]) ? slow[k] + 1 : 0;
+                if (slow[k] >= 6) { done[k] = 1; status[k] = TDDA_SOLVE_STAGNATED; }
+            }
+            prev[k] = S.err;
+            all &= (done[k] != 0);
+        }
+        if (all) break;
+        // inner right-hand sides R^ = S R / ||R|| (finished ones: zero)
+        std::fill(h, h + 3 * (size_t)nrhs, 0.0);
+        for (int k = 0; k < nrhs; ++k) {
+            if (done[k]) continue;
+            const SolverState &S = w.st_res_host[k];
+            const double rn = S.err * S.enorm;
+            h[k] = 1.0 / rn;
+            h[nrhs + k] = rn;
+            h[2 * nrhs + k] = std::max(0.5 * tol / S.err, o.floor);  // reduction this cycle must reach
+        }
+        TDDA_CUDA_TRY(cudaMemcpyAsync(w.d_part, h, sizeof(double) * 3 * nrhs, cudaMemcpyHostToDevice, s));
+        launch_to_inner<C>(n, w.nbox, nrhs, w.dstride, w.Rm, w.d_part, w.sc64, w.R, s);
+        // V[0] = R^ / ||R^||
+        gs_update(gw, 0, gw.h, 0, w.R, true, s);  // norms only (no basis vectors)
+        scale_vec(gw, gw.nrm + nrhs, w.R, basis(gw, 0), s);
+        TDDA_CUDA_TRY(cudaMemcpyAsync(gw.h_host, gw.nrm, sizeof(double) * nrhs, cudaMemcpyDeviceToHost, s));
+        TDDA_CUDA_TRY(cudaStreamSynchronize(s));
+        for (int k = 0; k < nrhs; ++k) beta[k] = reinterpret_cast<const double *>(gw.h_host)[k];
+        if (roots.empty()) {
+            // the polynomial: Arnoldi steps of the inner operator on the first
+            // residual of the first unfinished right-hand side
+            int k0 = 0;
+            while (k0 < nrhs && done[k0]) ++k0;
+            const int dd = std::min(d, m);
+            std::vector<cplx> Hb((size_t)(dd + 1) * dd, cplx(0.0));
+            int got = dd;
+            for (int j = 0; j < dd; ++j) {
+                st = arnoldi_step(gw, j, op_plain, Hcol, s);
+                if (st != TDDA_OK) return st;
+                for (int i = 0; i <= j + 1; ++i) Hb[i + (size_t)j * (dd + 1)] = Hcol[k0][i];
+                for (int k = 0; k < nrhs; ++k) mv[k] += 1;
+                if (std::abs(Hcol[k0][j + 1]) <= 1e-14 * std::abs(Hcol[k0][j])) { got = j + 1; break; }
+            }
+            std::vector<cplx> th, Hg((size_t)(got + 1) * got);
+            for (int j = 0; j < got; ++j)
+                for (int i = 0; i <= got; ++i) Hg[i + (size_t)j * (got + 1)] = Hb[i + (size_t)j * (dd + 1)];
+            if (!harmonic_ritz(Hg.data(), got, got + 1, th)) {
+                set_error("polynomial preconditioner: harmonic Ritz values did not converge");
+                return TDDA_ERR_BREAKDOWN;
+            }
+            for (auto &t : th)
+                if (std::abs(t) == 0.0 || !std::isfinite(t.real()) || !std::isfinite(t.imag())) {
+                    set_error("polynomial preconditioner: a harmonic Ritz value is zero or not finite");
+                    return TDDA_ERR_BREAKDOWN;
+                }
+            leja_order(th);
+            roots = th;
+            // V[0] is unchanged by those steps; the cycle overwrites V[1..]
+        }
+        // one GMRES cycle on Ah p(Ah)
+        for (int k = 0; k < nrhs; ++k) qr[k].reset(m, beta[k]);
+        int kk = 0;
+        for (int j = 0; j < m; ++j) {
+            st = arnoldi_step(gw, j, op_poly, Hcol, s);
+            if (st != TDDA_OK) return st;
+            kk = j + 1;
+            bool reached = true;
+            for (int k = 0; k < nrhs; ++k) {
+                if (done[k]) continue;
+                const double est = qr[k].add(j, Hcol[k]);
+                mv[k] += (long long)roots.size();
+                steps[k] += 1;
+                if (!(est <= h[2 * nrhs + k] * beta[k]) && mv[k] < max_iter) reached = false;
+            }
+            if (reached) break;
+        }
+        // correction u = V y, D = p(Ah) u, X += ||R|| S D
+        std::vector<double2> coef((size_t)nrhs * kk, make_double2(0.0, 0.0));
+        for (int k = 0; k < nrhs; ++k) {
+            if (done[k]) continue;
+            std::vector<cplx> y;
+            qr[k].solve(kk, y);
+            for (int i = 0; i < kk; ++i) coef[(size_t)k * kk + i] = make_double2(y[i].real(), y[i].imag());
+            cycles[k] += 1;
+        }
+        TDDA_CUDA_TRY(cudaMemcpyAsync(gw.coef, coef.data(), sizeof(double2) * coef.size(), cudaMemcpyHostToDevice, s));
+        count_launches(1);
+        launch_dep(k_lincomb<C>, dim3(gs_blocks(n), 1, nrhs), dim3(kGsThreads), sizeof(double2) * kk, s, n, kk,
+                   (const C *)gw.V, (size_t)n * nrhs, (size_t)n, (const double2 *)gw.coef, kk, w.D);
+        for (int i = 0; i < (int)roots.size(); ++i) {
+            const cplx c = 1.0 / roots[i];
+            st = poly_factor<C>(*w.op, w.sc, w.al, i == 0 ? w.D : gw.W, gw.W, gw.Y, i == 0, nullptr, nullptr,
+                                make_double2(c.real(), c.imag()), nrhs, w.dstride, s);
+            if (st != TDDA_OK) return st;
+        }
+        for (int k = 0; k < nrhs; ++k)
+            if (!done[k]) mv[k] += (long long)roots.size();
+        launch_axpy_inner<C>(n, w.nbox, nrhs, w.dstride, w.d_part + nrhs, w.sc64, gw.Y, X, s);
+        TDDA_CUDA_TRY(cudaGetLastError());
+    }
+    if (info)
+        for (int k = 0; k < nrhs; ++k) {
+            info[k].iterations = steps[k];
+            info[k].error = err[k];
+            info[k].status = status[k];
+            info[k].refinements = cycles[k];
+            info[k].inner_iterations = (int)std::min<long long>(mv[k], 2147483647LL);
+            info[k].true_error = err[k];
+        }
+    return TDDA_OK;
+}
+
+template struct GmresWork<float2>;
+template struct GmresWork<double2>;
+template tdda_status pgmres_solve<float2>(const RefineWork<float2> &, GmresWork<float2> &, const double2 *, double2 *,
+                                          int, bool, int, double, const GmresOptions &, tdda_solve_info *);
+template tdda_status pgmres_solve<double2>(const RefineWork<double2> &, GmresWork<double2> &, const double2 *,
+                                           double2 *, int, bool, int, double, const GmresOptions &,
+                                           tdda_solve_info *);
+
+}  // namespace tdda

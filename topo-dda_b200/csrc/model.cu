@@ -20,6 +20,7 @@
 #include "model_view.cuh"
 #include "operator.cuh"
 #include "refine.cuh"
+#include "gmres.cuh"
 
 namespace tdda {
 
@@ -430,6 +431,11 @@ struct tdda_model {
     int obs_lo[3]{}, obs_n[3]{};
     double2 *Einc_obs = nullptr; // [nobs][3]
     double2 *Eobs = nullptr;     // [nobs][3]
+    // solver of later solves: 0 BiCGSTAB, 1 polynomial-preconditioned GMRES
+    int solver = 0;
+    GmresOptions gopt{};
+    GmresWork<double2> gw64;
+    GmresWork<float2> gw32;
     // stats
     double lattice_ms = 0, fft_ms = 0;
     long long device_bytes = 0;
@@ -439,6 +445,8 @@ struct tdda_model {
         op32.release();
         kv.release();
         kv32.release();
+        gw64.release();
+        gw32.release();
         void *bufs[] = {d_cell, d_mask, d_rho,  al,  diel, al32,  Einc, P,     Eres,  ext,   bufB,     bufX,
                         Rm,     R32,    D32,    st_res, d_part, R64, D64,  sc64, alS64, sc32, alS32, d_obs,
                         Gobs,   Einc_obs, Eobs};
@@ -658,10 +666,42 @@ static tdda_status solve_refined(tdda_model *m, const double2 *B, double2 *X, in
     return refine_solve<C>(w, B, X, nrhs, x0_zero, max_iter, tol, info);
 }
 
+static GmresWork<float2> &gmres_work(tdda_model *m, float2 *) { return m->gw32; }
+static GmresWork<double2> &gmres_work(tdda_model *m, double2 *) { return m->gw64; }
+
+// Polynomial-preconditioned GMRES in complex128 refinement, inner solves in C
+// (complex64 for mixed precision), always Jacobi-scaled.
+template <typename C>
+static tdda_status solve_pgmres(tdda_model *m, const double2 *B, double2 *X, int nrhs, bool x0_zero, int max_iter,
+                                double tol, tdda_solve_info *info) {
+    TRY(ensure_refine(m, nrhs, (C *)nullptr));
+    GmresWork<C> &gw = gmres_work(m, (C *)nullptr);
+    if (gw.nrhs != nrhs || gw.restart != m->gopt.restart || gw.degree != m->gopt.degree) {
+        gw.release();
+        TRY(gw.init(3 * m->nbox, nrhs, m->gopt.restart, m->gopt.degree));
+    }
+    const int saved = m->precond;
+    m->precond = 1;
+    RefineWork<C> w = refine_work(m, (C *)nullptr);
+    m->precond = saved;
+    w.op64 = &m->op; w.al64 = m->al; w.sc64 = m->sc64;
+    w.Rm = m->Rm; w.st_res = m->st_res; w.st_res_host = m->st_res_host;
+    w.d_part = m->d_part; w.h_part = m->h_part;
+    w.nbox = m->nbox; w.s = m->stream;
+    GmresOptions o = m->gopt;
+    o.floor = sizeof(C) == sizeof(float2) ? 2e-6 : 0.0;
+    return pgmres_solve<C>(w, gw, B, X, nrhs, x0_zero, max_iter, tol, o, info);
+}
+
 static tdda_status solve_internal(tdda_model *m, const double2 *B, double2 *X, int nrhs, bool x0_zero,
                                   int max_iter, double tol, tdda_solve_info *info) {
     if (max_iter < 0) return bad("max_iter must be >= 0");
     if (!(tol >= 0.0)) return bad("tolerance must be >= 0");
+    if (m->solver == 1) {
+        if (m->precision == TDDA_PREC_MIXED)
+            return solve_pgmres<float2>(m, B, X, nrhs, x0_zero, max_iter, tol, info);
+        return solve_pgmres<double2>(m, B, X, nrhs, x0_zero, max_iter, tol, info);
+    }
     if (m->precision == TDDA_PREC_MIXED)
         return solve_refined<float2>(m, B, X, nrhs, x0_zero, max_iter, tol, info);
     if (m->precond != 0) return solve_refined<double2>(m, B, X, nrhs, x0_zero, max_iter, tol, info);
@@ -1227,6 +1267,19 @@ tdda_status tdda_set_precision(tdda_model *m, int precision) {
         return TDDA_OK;
     }
     return bad("precision must be 0 or 1");
+}
+
+tdda_status tdda_set_solver(tdda_model *m, int kind, int degree, int restart) {
+    if (m == nullptr) return bad("null model");
+    if (kind != 0 && kind != 1) return bad("solver must be 0 (BiCGSTAB) or 1 (polynomial-preconditioned GMRES)");
+    if (kind == 1) {
+        if (degree < 1 || degree > 64) return bad("polynomial degree must be in [1, 64]");
+        if (restart < 1 || restart > 256) return bad("GMRES restart must be in [1, 256]");
+        m->gopt.degree = degree;
+        m->gopt.restart = restart;
+    }
+    m->solver = kind;
+    return TDDA_OK;
 }
 
 tdda_status tdda_set_preconditioner(tdda_model *m, int kind) {

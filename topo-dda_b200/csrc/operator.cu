@@ -793,6 +793,30 @@ template <typename C> struct EpiMatvec : EpiBase<C> {
     __device__ void operator()(int, const double2 *) const {}
 };
 
+// One factor of the polynomial preconditioner of the GMRES solver (gmres.cuh):
+// Ar = conv + al o r (the operator the passes apply), r' = r - c Ar, and
+// y = c r (first) or y += c r when y is given; r' goes to rout (may alias rin:
+// every element is read and written by one thread), or wout = v0 - r'.
+template <typename C> struct EpiPoly : EpiBase<C> {
+    static constexpr int NQ = 0;
+    const C *rin, *al, *v0;
+    C *rout, *y, *wout;
+    double2 c;
+    int first;
+    __device__ bool skip(int) const { return false; }
+    __device__ void apply(int rhs, int comp, long long cell, C conv, double2 *) const {
+        const size_t i = this->idx(rhs, comp, cell);
+        const C r = rin[i];
+        const C Ar = this->masked(rhs, cell, conv) + __ldg(al + this->didx(rhs, cell)) * r;
+        const C cc = from_d<C>(c);
+        const C rn = r - cc * Ar;
+        if (y != nullptr) y[i] = first ? cc * r : y[i] + cc * r;
+        if (wout != nullptr) wout[i] = __ldg(v0 + i) - rn;
+        else if (rout != nullptr) rout[i] = rn;
+    }
+    __device__ void operator()(int, const double2 *) const {}
+};
+
 // r = B - (A x0 + al o x0); r0 = r;  sums: r0.r, ||B||^2   src/DDAModel.cpp:925-928
 template <typename C> struct EpiInit : EpiBase<C> {
     static constexpr int NQ = 2;
@@ -1093,6 +1117,7 @@ template <typename C> static void set_smem_attrs(int yz, int x) {
     cudaFuncSetAttribute(k_fwd_zy<C, ProPF<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, yz);
     cudaFuncSetAttribute(k_inv_yz<C, EpiAtF<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, yz);
     cudaFuncSetAttribute(k_inv_yz<C, EpiMatvec<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, yz);
+    cudaFuncSetAttribute(k_inv_yz<C, EpiPoly<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, yz);
     cudaFuncSetAttribute(k_inv_yz<C, EpiInit<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, yz);
     cudaFuncSetAttribute(k_inv_yz<C, EpiAp<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, yz);
     cudaFuncSetAttribute(k_inv_yz<C, EpiAt<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, yz);
@@ -1125,6 +1150,7 @@ template <typename C> static void set_smem_attrs(int yz, int x) {
     cudaFuncSetAttribute(k_fwd_zy_fast<C, a, b, ProPF<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemFast);     \
     cudaFuncSetAttribute(k_inv_yz_fast<C, a, b, EpiAtF<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemFast);    \
     cudaFuncSetAttribute(k_inv_yz_fast<C, a, b, EpiMatvec<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemFast); \
+    cudaFuncSetAttribute(k_inv_yz_fast<C, a, b, EpiPoly<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemFast);   \
     cudaFuncSetAttribute(k_inv_yz_fast<C, a, b, EpiInit<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemFast);   \
     cudaFuncSetAttribute(k_inv_yz_fast<C, a, b, EpiAp<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemFast);     \
     cudaFuncSetAttribute(k_inv_yz_fast<C, a, b, EpiAt<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemFast);
@@ -1137,6 +1163,7 @@ template <typename C> static void set_smem_attrs(int yz, int x) {
     cudaFuncSetAttribute(k_fwd_zy_reg<C, a, b, ProPF<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemFast);      \
     cudaFuncSetAttribute(k_inv_yz_reg<C, a, b, EpiAtF<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemFast);     \
     cudaFuncSetAttribute(k_inv_yz_reg<C, a, b, EpiMatvec<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemFast);  \
+    cudaFuncSetAttribute(k_inv_yz_reg<C, a, b, EpiPoly<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemFast);    \
     cudaFuncSetAttribute(k_inv_yz_reg<C, a, b, EpiInit<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemFast);    \
     cudaFuncSetAttribute(k_inv_yz_reg<C, a, b, EpiAp<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemFast);      \
     cudaFuncSetAttribute(k_inv_yz_reg<C, a, b, EpiAt<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemFast);
@@ -1323,6 +1350,49 @@ tdda_status ConvOperator<C>::apply(const C *x, C *y, const C *al, int nrhs, cuda
     TDDA_CUDA_TRY(cudaGetLastError());
     return TDDA_OK;
 }
+
+template <typename C>
+tdda_status apply_scaled(ConvOperator<C> &op, const C *sc, const C *al, const C *x, C *y, int nrhs, size_t dstride,
+                         cudaStream_t s) {
+    if (nrhs > op.nrhs_cap) { set_error("nrhs exceeds operator capacity"); return TDDA_ERR_BAD_ARG; }
+    ConvGeom gg;
+    if (!geom_for(op, nrhs, gg)) { set_error("batch does not fit the x pass"); return TDDA_ERR_UNSUPPORTED; }
+    ProLoad<C> pro{};
+    pro.nbox = op.g.nbox; pro.x = x; pro.st = nullptr; pro.sc = sc; pro.dstride = dstride;
+    EpiMatvec<C> epi{};
+    epi.nbox = op.g.nbox; epi.mask = op.mask; epi.y = y; epi.x = x; epi.al = al; epi.sc = sc; epi.dstride = dstride;
+    run_conv(op, gg, nrhs, pro, epi, nullptr, s);
+    TDDA_CUDA_TRY(cudaGetLastError());
+    return TDDA_OK;
+}
+
+template <typename C>
+tdda_status poly_factor(ConvOperator<C> &op, const C *sc, const C *al, const C *rin, C *rout, C *y, bool first,
+                        const C *v0, C *wout, double2 c, int nrhs, size_t dstride, cudaStream_t s) {
+    if (nrhs > op.nrhs_cap) { set_error("nrhs exceeds operator capacity"); return TDDA_ERR_BAD_ARG; }
+    ConvGeom gg;
+    if (!geom_for(op, nrhs, gg)) { set_error("batch does not fit the x pass"); return TDDA_ERR_UNSUPPORTED; }
+    ProLoad<C> pro{};
+    pro.nbox = op.g.nbox; pro.x = rin; pro.st = nullptr; pro.sc = sc; pro.dstride = dstride;
+    EpiPoly<C> epi{};
+    epi.nbox = op.g.nbox; epi.mask = op.mask; epi.sc = sc; epi.dstride = dstride;
+    epi.rin = rin; epi.al = al; epi.v0 = v0; epi.rout = rout; epi.y = y; epi.wout = wout; epi.c = c;
+    epi.first = first ? 1 : 0;
+    run_conv(op, gg, nrhs, pro, epi, nullptr, s);
+    TDDA_CUDA_TRY(cudaGetLastError());
+    return TDDA_OK;
+}
+
+template tdda_status apply_scaled<float2>(ConvOperator<float2> &, const float2 *, const float2 *, const float2 *,
+                                          float2 *, int, size_t, cudaStream_t);
+template tdda_status apply_scaled<double2>(ConvOperator<double2> &, const double2 *, const double2 *,
+                                           const double2 *, double2 *, int, size_t, cudaStream_t);
+template tdda_status poly_factor<float2>(ConvOperator<float2> &, const float2 *, const float2 *, const float2 *,
+                                         float2 *, float2 *, bool, const float2 *, float2 *, double2, int, size_t,
+                                         cudaStream_t);
+template tdda_status poly_factor<double2>(ConvOperator<double2> &, const double2 *, const double2 *,
+                                          const double2 *, double2 *, double2 *, bool, const double2 *, double2 *,
+                                          double2, int, size_t, cudaStream_t);
 
 template <typename C>
 tdda_status apply_external_scratch(const ConvOperator<C> &op, C *T_ext, const C *x, C *y, const C *al,

@@ -267,6 +267,14 @@ class DDAModel:
         k = {"none": 0, "jacobi": 1}[kind]
         _lib.check(self._lib.tdda_set_preconditioner(self._handle, k))
 
+    def setSolver(self, kind, degree=24, restart=40):
+        """"bicgstab" (the reference's solver) or "pgmres": restarted GMRES on the
+        Jacobi-scaled operator times a polynomial of `degree` in it, one cycle of
+        `restart` steps per complex128 refinement step (for structures that fill
+        their periodic cell, where BiCGSTAB stalls)."""
+        k = {"bicgstab": 0, "pgmres": 1}[kind]
+        _lib.check(self._lib.tdda_set_solver(self._handle, k, int(degree), int(restart)))
+
     @staticmethod
     def kernel_launches():
         return int(_lib.load().tdda_kernel_launches())

@@ -173,6 +173,7 @@ SIGNATURES = {
     "tdda_lattice_offsets_device": (ctypes.c_int, [ctypes.c_void_p, _ip, _ip, ctypes.c_void_p, ctypes.c_void_p]),
     "tdda_set_precision": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "tdda_set_preconditioner": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "tdda_set_solver": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "tdda_set_observation_points": (ctypes.c_int, [ctypes.c_void_p, _ip, ctypes.c_int64]),
     "tdda_observation_field": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_int64]),
     "tdda_patch_objective": (ctypes.c_int, [ctypes.c_void_p, _dp]),
