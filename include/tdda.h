@@ -159,6 +159,31 @@ tdda_status tdda_set_densities(tdda_model *m, const double *rho, int64_t n);
  * runs one adjoint solve, grad: double[N]. */
 tdda_status tdda_gradient_densities(tdda_model *m, int max_iter, double tol, double *grad, int64_t n,
                                     tdda_solve_info *info);
+/* Device-pointer forms of tdda_set_densities / tdda_gradient_densities /
+ * tdda_patch_gradient for callers whose densities and gradients live on the
+ * GPU (the torch.autograd path): rho_dev and grad_dev are double[N] device
+ * arrays in dipole order; the work is ordered after, and the results are
+ * ready on, `stream` (NULL: the legacy default stream).  Setting densities
+ * checks them in [0, 1] (one small device-to-host read). */
+tdda_status tdda_set_densities_device(tdda_model *m, const double *rho_dev, void *stream);
+tdda_status tdda_gradient_densities_device(tdda_model *m, int max_iter, double tol, double *grad_dev, void *stream,
+                                           tdda_solve_info *info);
+tdda_status tdda_patch_gradient_device(tdda_model *m, int max_iter, double tol, double *grad_dev, void *stream,
+                                       tdda_solve_info *info);
+/* The design-density chain of the differentiation workload on the device (no
+ * reference counterpart; the reference's own in-plane filter and exponential
+ * projection are the tdda_filter_* entry points): raw_dev[x][y][z] (z
+ * fastest) -> filtered_dev[x][y][z] = radius-R cone filter (periodic in x and
+ * y, truncated and renormalised in z; 0 < R <= 6 cells) -> rho_dev (dipole
+ * order, x fastest) = tanh projection (beta, eta) clamped to [0, 1].  The
+ * backward pass maps dJ/drho (dipole order) to dJ/draw ([x][y][z]) given the
+ * forward's filtered field; scratch_dev holds nx*ny*nz doubles.  Work runs on
+ * `stream`. */
+tdda_status tdda_design_forward_device(int nx, int ny, int nz, double radius, double beta, double eta,
+                                       const double *raw_dev, double *filtered_dev, double *rho_dev, void *stream);
+tdda_status tdda_design_backward_device(int nx, int ny, int nz, double radius, double beta, double eta,
+                                        const double *filtered_dev, const double *grad_rho_dev, double *grad_raw_dev,
+                                        double *scratch_dev, void *stream);
 /* Observation-patch objective (no reference counterpart; the nearest is
  * ObjPointEDDAModel, src/ObjDDAModel.cpp:20-100, and the off-structure branch
  * of DDAModel::solve_E, src/DDAModel.cpp:1154-1179): points xyz[3*nobs] in grid

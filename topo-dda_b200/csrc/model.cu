@@ -69,6 +69,30 @@ __global__ void k_scatter(int nrhs, long long N, long long nbox, const long long
     }
 }
 
+// count of densities outside [0, 1] (NaN included)
+__global__ void k_rho_check(long long N, const double *__restrict__ rho, unsigned *__restrict__ bad) {
+    unsigned c = 0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
+        const double v = rho[i];
+        if (!(v >= 0.0 && v <= 1.0)) ++c;
+    }
+    if (c) atomicAdd(bad, c);
+}
+
+// density per cell from per-dipole densities (cells without a dipole keep 0)
+__global__ void k_rho_scatter(long long N, const long long *__restrict__ cell_of, const double *__restrict__ rho,
+                              double *__restrict__ d_rho) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x)
+        d_rho[cell_of[i]] = rho[i];
+}
+
+// per-dipole values from per-cell values
+__global__ void k_cell_to_dipole(long long N, const long long *__restrict__ cell_of, const double *__restrict__ v,
+                                 double *__restrict__ out) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x)
+        out[i] = v[cell_of[i]];
+}
+
 __global__ void k_gather(int nrhs, long long N, long long nbox, const long long *__restrict__ cell_of,
                          const double2 *__restrict__ in, double2 *__restrict__ ext) {
     long long tot = (long long)nrhs * N * 3;
@@ -389,6 +413,7 @@ struct tdda_model {
     double E_int = 0.0;                   // objective state of the last calculateObjective
     bool per_dipole = false;              // densities set per dipole (tdda_set_densities)
     std::vector<double> rho_dipole;       // per-dipole densities when per_dipole
+    bool rho_host_stale = false;          // set on the device since: rho_dipole must be read back
     // device
     cudaStream_t stream = nullptr;
     ConvOperator<double2> op;
@@ -419,6 +444,8 @@ struct tdda_model {
     double2 a0{};                          // mean diagonal of the zero-offset tensor entry
     double2 *sc64 = nullptr, *alS64 = nullptr;
     float2 *sc32 = nullptr, *alS32 = nullptr;
+    double *d_grad = nullptr;              // per-cell gradient scratch
+    unsigned *d_flag = nullptr, *h_flag = nullptr;  // density check count (device, pinned)
     SolverState *st_res = nullptr, *st_res_host = nullptr;
     double *d_part = nullptr, *h_part = nullptr;
     // lattice inputs kept for later tensors (observation patches)
@@ -449,8 +476,9 @@ struct tdda_model {
         gw32.release();
         void *bufs[] = {d_cell, d_mask, d_rho,  al,  diel, al32,  Einc, P,     Eres,  ext,   bufB,     bufX,
                         Rm,     R32,    D32,    st_res, d_part, R64, D64,  sc64, alS64, sc32, alS32, d_obs,
-                        Gobs,   Einc_obs, Eobs};
+                        Gobs,   Einc_obs, Eobs, d_grad, d_flag};
         for (void *b : bufs) cudaFree(b);
+        cudaFreeHost(h_flag);
         cudaFreeHost(st_res_host);
         cudaFreeHost(h_part);
         if (stream) cudaStreamDestroy(stream);
@@ -1084,9 +1112,19 @@ tdda_status tdda_get_parameter_map(const tdda_model *m, int32_t *map, int64_t n)
     return TDDA_OK;
 }
 
-tdda_status tdda_get_dielectrics(const tdda_model *m, double *out, int64_t n) {
-    if (!m || !out) return bad("null argument");
-    if (n != 3LL * m->N) return bad("buffer must hold 3N values");
+tdda_status tdda_get_dielectrics(const tdda_model *cm, double *out, int64_t n) {
+    if (!cm || !out) return bad("null argument");
+    if (n != 3LL * cm->N) return bad("buffer must hold 3N values");
+    tdda_model *m = const_cast<tdda_model *>(cm);  // refreshes the host mirror of device-set densities
+    if (m->rho_host_stale) {
+        std::vector<double> cells(m->nbox);
+        TDDA_CUDA_TRY(cudaMemcpyAsync(cells.data(), m->d_rho, sizeof(double) * m->nbox, cudaMemcpyDeviceToHost,
+                                      m->stream));
+        TDDA_CUDA_TRY(cudaStreamSynchronize(m->stream));
+        m->rho_dipole.resize(m->N);
+        for (int i = 0; i < m->N; ++i) m->rho_dipole[i] = cells[m->cell_of[i]];
+        m->rho_host_stale = false;
+    }
     for (int i = 0; i < m->N; ++i) {
         double v = m->per_dipole ? m->rho_dipole[i] : m->parameters[m->geometryPara[i]];
         out[3 * i] = out[3 * i + 1] = out[3 * i + 2] = v;
@@ -1200,41 +1238,109 @@ tdda_status tdda_set_densities(tdda_model *m, const double *rho, int64_t n) {
     const bool old_pd = m->per_dipole;
     m->rho_dipole.assign(rho, rho + n);
     m->per_dipole = true;
+    const bool old_stale = m->rho_host_stale;
+    m->rho_host_stale = false;
     tdda_status s = update_alpha(m);
     if (s != TDDA_OK) {
         m->rho_dipole = old;
         m->per_dipole = old_pd;
+        m->rho_host_stale = old_stale;
     }
     return s;
 }
 
-tdda_status tdda_gradient_densities(tdda_model *m, int max_iter, double tol, double *grad, int64_t n,
-                                    tdda_solve_info *info) {
-    if (!m || !grad) return bad("null argument");
-    if (n != m->N) return bad("gradient buffer must hold N values");
+// Makes `to` wait for the work queued so far on `from`.
+static tdda_status join_streams(cudaStream_t from, cudaStream_t to) {
+    cudaEvent_t ev;
+    TDDA_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    cudaError_t e1 = cudaEventRecord(ev, from);
+    cudaError_t e2 = e1 == cudaSuccess ? cudaStreamWaitEvent(to, ev, 0) : e1;
+    cudaEventDestroy(ev);
+    TDDA_CUDA_TRY(e2);
+    return TDDA_OK;
+}
+
+static tdda_status ensure_grad_scratch(tdda_model *m) {
+    if (m->d_grad == nullptr) TDDA_CUDA_TRY(cudaMalloc(&m->d_grad, sizeof(double) * m->nbox));
+    if (m->d_flag == nullptr) {
+        TDDA_CUDA_TRY(cudaMalloc(&m->d_flag, sizeof(unsigned)));
+        TDDA_CUDA_TRY(cudaMallocHost(&m->h_flag, sizeof(unsigned)));
+    }
+    return TDDA_OK;
+}
+
+tdda_status tdda_set_densities_device(tdda_model *m, const double *rho_dev, void *stream) {
+    if (!m || !rho_dev) return bad("null argument");
+    TRY(ensure_grad_scratch(m));
+    cudaStream_t user = (cudaStream_t)stream;
+    TRY(join_streams(user, m->stream));
+    TDDA_CUDA_TRY(cudaMemsetAsync(m->d_flag, 0, sizeof(unsigned), m->stream));
+    count_launches(1);
+    k_rho_check<<<grid_for(m->N), 256, 0, m->stream>>>(m->N, rho_dev, m->d_flag);
+    TDDA_CUDA_TRY(cudaMemcpyAsync(m->h_flag, m->d_flag, sizeof(unsigned), cudaMemcpyDeviceToHost, m->stream));
+    TDDA_CUDA_TRY(cudaStreamSynchronize(m->stream));
+    if (*m->h_flag != 0) return bad("design density outside [0, 1]");
+    count_launches(3);
+    k_rho_scatter<<<grid_for(m->N), 256, 0, m->stream>>>(m->N, m->d_cell, rho_dev, m->d_rho);
+    k_alpha<<<grid_for(m->nbox), 256, 0, m->stream>>>(m->nbox, m->d_rho, m->d_mask, m->ap, m->al, m->al32, m->diel);
+    k_jacobi<<<grid_for(m->nbox), 256, 0, m->stream>>>(m->nbox, m->al, m->d_mask, m->a0, m->sc64, m->alS64,
+                                                        m->sc32, m->alS32);
+    TDDA_CUDA_TRY(cudaGetLastError());
+    m->per_dipole = true;
+    m->rho_host_stale = true;
+    return join_streams(m->stream, user);
+}
+
+// The exact adjoint gradient of IntegratedE per cell into m->d_grad.
+static tdda_status gradient_cells(tdda_model *m, int max_iter, double tol, tdda_solve_info *info) {
     double S;
     TRY(objective_sum(m, m->P, &S));
     if (!(S > 0.0)) return bad("objective sum is zero: solve first");
     TRY(ensure_batch(m, 1));
+    TRY(ensure_grad_scratch(m));
     const long long nbox = m->nbox;
     k_adjoint_rhs<<<grid_for(nbox), 256, 0, m->stream>>>(nbox, m->P, m->al, m->d_mask, m->powNum, S, m->bufB);
     count_launches(1);
     TDDA_CUDA_TRY(cudaGetLastError());
     tdda_solve_info inf{};
     TRY(solve_internal(m, m->bufB, m->bufX, 1, true, max_iter, tol, &inf));
-    double *g = nullptr;
-    TDDA_CUDA_TRY(cudaMalloc(&g, sizeof(double) * nbox));
-    std::unique_ptr<void, void (*)(void *)> gg(g, [](void *p) { cudaFree(p); });
     k_grad_analytic<<<grid_for(nbox), 256, 0, m->stream>>>(nbox, m->d_rho, m->d_mask, m->P, m->al, m->diel, m->bufX,
-                                                           m->ap, m->powNum, S, g);
+                                                           m->ap, m->powNum, S, m->d_grad);
     count_launches(1);
     TDDA_CUDA_TRY(cudaGetLastError());
-    std::vector<double> h(nbox);
-    TDDA_CUDA_TRY(cudaMemcpyAsync(h.data(), g, sizeof(double) * nbox, cudaMemcpyDeviceToHost, m->stream));
-    TDDA_CUDA_TRY(cudaStreamSynchronize(m->stream));
-    for (int i = 0; i < m->N; ++i) grad[i] = h[m->cell_of[i]];
     if (info) *info = inf;
     return TDDA_OK;
+}
+
+static tdda_status cells_to_host(tdda_model *m, const double *cells, double *out) {
+    std::vector<double> h(m->nbox);
+    TDDA_CUDA_TRY(cudaMemcpyAsync(h.data(), cells, sizeof(double) * m->nbox, cudaMemcpyDeviceToHost, m->stream));
+    TDDA_CUDA_TRY(cudaStreamSynchronize(m->stream));
+    for (int i = 0; i < m->N; ++i) out[i] = h[m->cell_of[i]];
+    return TDDA_OK;
+}
+
+static tdda_status cells_to_device(tdda_model *m, const double *cells, double *out_dev, cudaStream_t user) {
+    count_launches(1);
+    k_cell_to_dipole<<<grid_for(m->N), 256, 0, m->stream>>>(m->N, m->d_cell, cells, out_dev);
+    TDDA_CUDA_TRY(cudaGetLastError());
+    return join_streams(m->stream, user);
+}
+
+tdda_status tdda_gradient_densities(tdda_model *m, int max_iter, double tol, double *grad, int64_t n,
+                                    tdda_solve_info *info) {
+    if (!m || !grad) return bad("null argument");
+    if (n != m->N) return bad("gradient buffer must hold N values");
+    TRY(gradient_cells(m, max_iter, tol, info));
+    return cells_to_host(m, m->d_grad, grad);
+}
+
+tdda_status tdda_gradient_densities_device(tdda_model *m, int max_iter, double tol, double *grad_dev, void *stream,
+                                           tdda_solve_info *info) {
+    if (!m || !grad_dev) return bad("null argument");
+    TRY(join_streams((cudaStream_t)stream, m->stream));
+    TRY(gradient_cells(m, max_iter, tol, info));
+    return cells_to_device(m, m->d_grad, grad_dev, (cudaStream_t)stream);
 }
 
 tdda_status tdda_profile_matvec(tdda_model *m, int precision, int nrhs, int iters, double *ms_matvec,
@@ -1380,12 +1486,11 @@ tdda_status tdda_patch_objective(tdda_model *m, double *out) {
     return TDDA_OK;
 }
 
-tdda_status tdda_patch_gradient(tdda_model *m, int max_iter, double tol, double *grad, int64_t n,
-                                tdda_solve_info *info) {
-    if (!m || !grad) return bad("null argument");
-    if (n != m->N) return bad("gradient buffer must hold N values");
+// The exact adjoint gradient of the patch objective per cell into m->d_grad.
+static tdda_status patch_gradient_cells(tdda_model *m, int max_iter, double tol, tdda_solve_info *info) {
     TRY(patch_field(m));
     TRY(ensure_batch(m, 1));
+    TRY(ensure_grad_scratch(m));
     const long long nbox = m->nbox;
     count_launches(1);
     k_patch_adjoint_rhs<<<grid_for(nbox), 256, 0, m->stream>>>(m->nobs, m->d_obs, patch_geo(m), m->d_mask, nbox,
@@ -1393,18 +1498,27 @@ tdda_status tdda_patch_gradient(tdda_model *m, int max_iter, double tol, double 
     TDDA_CUDA_TRY(cudaGetLastError());
     tdda_solve_info inf{};
     TRY(solve_internal(m, m->bufB, m->bufX, 1, true, max_iter, tol, &inf));
-    double *g = nullptr;
-    TDDA_CUDA_TRY(cudaMalloc(&g, sizeof(double) * nbox));
-    std::unique_ptr<void, void (*)(void *)> gg(g, [](void *p) { cudaFree(p); });
     count_launches(1);
-    k_grad_implicit<<<grid_for(nbox), 256, 0, m->stream>>>(nbox, m->d_mask, m->P, m->diel, m->bufX, m->ap, g);
+    k_grad_implicit<<<grid_for(nbox), 256, 0, m->stream>>>(nbox, m->d_mask, m->P, m->diel, m->bufX, m->ap, m->d_grad);
     TDDA_CUDA_TRY(cudaGetLastError());
-    std::vector<double> h(nbox);
-    TDDA_CUDA_TRY(cudaMemcpyAsync(h.data(), g, sizeof(double) * nbox, cudaMemcpyDeviceToHost, m->stream));
-    TDDA_CUDA_TRY(cudaStreamSynchronize(m->stream));
-    for (int i = 0; i < m->N; ++i) grad[i] = h[m->cell_of[i]];
     if (info) *info = inf;
     return TDDA_OK;
+}
+
+tdda_status tdda_patch_gradient(tdda_model *m, int max_iter, double tol, double *grad, int64_t n,
+                                tdda_solve_info *info) {
+    if (!m || !grad) return bad("null argument");
+    if (n != m->N) return bad("gradient buffer must hold N values");
+    TRY(patch_gradient_cells(m, max_iter, tol, info));
+    return cells_to_host(m, m->d_grad, grad);
+}
+
+tdda_status tdda_patch_gradient_device(tdda_model *m, int max_iter, double tol, double *grad_dev, void *stream,
+                                       tdda_solve_info *info) {
+    if (!m || !grad_dev) return bad("null argument");
+    TRY(join_streams((cudaStream_t)stream, m->stream));
+    TRY(patch_gradient_cells(m, max_iter, tol, info));
+    return cells_to_device(m, m->d_grad, grad_dev, (cudaStream_t)stream);
 }
 
 }  // extern "C"

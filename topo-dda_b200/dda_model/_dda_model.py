@@ -204,6 +204,25 @@ class DDAModel:
         v = _f64(rho, self.N, "densities")
         _lib.check(self._lib.tdda_set_densities(self._handle, _dp(v), v.size))
 
+    def setDensitiesDevice(self, rho_ptr, stream=None):
+        """Per-dipole densities from a device array (double[N], dipole order),
+        ordered after `stream`."""
+        _lib.check(self._lib.tdda_set_densities_device(self._handle, rho_ptr, stream))
+
+    def gradientDensitiesDevice(self, grad_ptr, max_iter=100000, tol=1e-10, stream=None):
+        """gradientDensities into a device array (double[N], dipole order), ready on `stream`."""
+        info = _lib.SolveInfo()
+        _lib.check(self._lib.tdda_gradient_densities_device(self._handle, int(max_iter), float(tol), grad_ptr,
+                                                            stream, ctypes.byref(info)))
+        self.last_adjoint = info.as_dict()
+
+    def patchGradientDevice(self, grad_ptr, max_iter=100000, tol=1e-10, stream=None):
+        """patchGradient into a device array (double[N], dipole order), ready on `stream`."""
+        info = _lib.SolveInfo()
+        _lib.check(self._lib.tdda_patch_gradient_device(self._handle, int(max_iter), float(tol), grad_ptr,
+                                                        stream, ctypes.byref(info)))
+        self.last_adjoint = info.as_dict()
+
     def gradientDensities(self, max_iter=100000, tol=1e-10):
         """Exact adjoint gradient of the objective w.r.t. every dipole density
         (uses the polarisation of the last solve)."""

@@ -174,6 +174,18 @@ SIGNATURES = {
     "tdda_set_precision": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "tdda_set_preconditioner": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "tdda_set_solver": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "tdda_set_densities_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "tdda_gradient_densities_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_double,
+                                                      ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(SolveInfo)]),
+    "tdda_patch_gradient_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_double,
+                                                  ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(SolveInfo)]),
+    "tdda_design_forward_device": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                                  ctypes.c_double, ctypes.c_double, ctypes.c_void_p,
+                                                  ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "tdda_design_backward_device": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                                   ctypes.c_double, ctypes.c_double, ctypes.c_void_p,
+                                                   ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                                   ctypes.c_void_p]),
     "tdda_set_observation_points": (ctypes.c_int, [ctypes.c_void_p, _ip, ctypes.c_int64]),
     "tdda_observation_field": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_int64]),
     "tdda_patch_objective": (ctypes.c_int, [ctypes.c_void_p, _dp]),
