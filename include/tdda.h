@@ -49,9 +49,9 @@ typedef struct tdda_model tdda_model;
 /* Constructor arguments of DDAModel (python_bindings/PythonBindings.cpp:19-46),
  * minus the arrays, which tdda_model_create takes separately. */
 typedef struct {
-    double beta_min, beta_max, ita;   /* filter: accepted, unused (disabled on every Python path) */
+    double beta_min, beta_max, ita;   /* legacy filter: projection schedule (src/FilterOption.cpp:5-21) */
     const char *beta_type;
-    int use_filter;                   /* must be 0: the legacy filter is not on this path */
+    int use_filter;                   /* the legacy filter (tdda_filter_*), src/DDAModel.cpp:255-264 */
     const char *symmetry_type;        /* "None" or "4fold" (src/DDAModel.cpp:163-173) */
     double symmetry_axis[2];
     int is_periodic;
@@ -72,6 +72,11 @@ typedef struct {
     double integral_delta;
     int verbose;
     int precision;                    /* tdda_precision */
+    /* filterIterations / filterRadii of the constructor: the legacy filter
+     * (use_filter != 0) uses filter_radii[0] (src/FilterOption.cpp:12-14) */
+    const int32_t *filter_iterations;
+    const double *filter_radii;
+    int n_filters;
 } tdda_params;
 
 typedef struct {
@@ -159,6 +164,22 @@ tdda_status tdda_set_densities(tdda_model *m, const double *rho, int64_t n);
  * runs one adjoint solve, grad: double[N]. */
 tdda_status tdda_gradient_densities(tdda_model *m, int max_iter, double tol, double *grad, int64_t n,
                                     tdda_solve_info *info);
+/* The reference's legacy design filter, for models created with use_filter
+ * (in the reference reachable from C++ only).  tdda_filter_update is
+ * DDAModel::UpdateStr (src/DDAModel.cpp:774-838) followed by the
+ * polarisability update (UpdateAlpha): the raw parameters take `step`
+ * (clamped to [0, 1]), are averaged with the in-plane cone weights of
+ * src/DDAModel.cpp:580-712 (radius filter_radii[0], periodic images when
+ * is_periodic) and projected by SmoothDensity (src/FilterOption.cpp:48-62) at
+ * the beta the schedule gives for (it, max_it) (src/FilterOption.cpp:23-45).
+ * tdda_filter_gradients is DDAModel::gradients_filtered
+ * (src/DDAModel.cpp:354-396).  tdda_filter_state returns the raw and filtered
+ * parameters and the current beta (get_Para_origin / get_Para_filtered /
+ * get_beta, src/DDAModel.cpp:1258-1360).  All arrays double[NFpara];
+ * TDDA_ERR_STATE without use_filter. */
+tdda_status tdda_filter_update(tdda_model *m, const double *step, int64_t n, int it, int max_it);
+tdda_status tdda_filter_gradients(tdda_model *m, const double *grad, int64_t n, int it, int max_it, double *out);
+tdda_status tdda_filter_state(tdda_model *m, double *raw, double *filtered, int64_t n, double *beta);
 /* Device-pointer forms of tdda_set_densities / tdda_gradient_densities /
  * tdda_patch_gradient for callers whose densities and gradients live on the
  * GPU (the torch.autograd path): rho_dev and grad_dev are double[N] device

@@ -25,6 +25,11 @@ oracle function                             reference (path within Topo-DDA)
 ``OracleModel.calculate_objective``         src/ObjDDAModel.cpp:103-218 (IntegratedE)
 ``OracleModel.calculate_gradients``         src/DDAModel.cpp:398-578
 ``OracleModel.dense_operator``              (dense 3N x 3N form of the same operator)
+``beta_schedule``                           src/FilterOption.cpp:23-45, src/Tools.cpp:473-516
+``smooth_density`` / ``smooth_density_d``   src/FilterOption.cpp:48-62, src/DDAModel.cpp:340-352
+``LegacyFilter`` (weights)                  src/DDAModel.cpp:66-77,580-712
+``LegacyFilter.update``                     src/DDAModel.cpp:774-838 (filter branch)
+``LegacyFilter.gradients``                  src/DDAModel.cpp:354-396
 ==========================================  ======================================
 
 Parity pins: ``tests/test_oracle_golden.py`` checks this oracle against the
@@ -609,3 +614,122 @@ def reference_fixture(data_dir):
         E0=1.0, n_E0=[1, 0, 0], lam=542.0, material=mats, nback=math.sqrt(1.01), MAXm=50,
         MAXn=50, Lm=22, Ln=22, matrixAMethodName="FCD", d=15.0, sineIntegralValues=si,
         cosineIntegralValues=ci, integralDelta=0.1, verbose=False)
+
+
+# ----------------------------------------------------------------------------
+# the reference's legacy design filter (in-plane cone filter + exponential
+# projection), reachable in the reference only from C++ (DDAModel::UpdateStr,
+# gradients_filtered)
+# ----------------------------------------------------------------------------
+
+def beta_schedule(beta_type, it, max_it, beta_min, beta_max):
+    """FilterOption::update_beta (src/FilterOption.cpp:23-45) with exp_update,
+    piecewise_update and linear_update (src/Tools.cpp:473-516)."""
+    x, xm = float(it), float(max_it)
+    if beta_type == "exp":
+        if x <= 300:
+            return beta_min + (beta_max - beta_min) * (math.pow(100.0, x / xm) - 1) / (100 - 1)
+        return 0.5
+    if beta_type == "piecewise":
+        if x <= 0.5 * xm:
+            return beta_min
+        if 0.5 * xm < x <= 0.7 * xm:
+            return beta_min + (beta_max - beta_min) / 5
+        if 0.7 * xm < x <= 0.8 * xm:
+            return beta_min + (beta_max - beta_min) / 2.5
+        return beta_max
+    if beta_type == "linear":
+        return beta_min + (beta_max - beta_min) * x / xm
+    raise RuntimeError("Unknown internal error")  # `throw 1` (src/FilterOption.cpp:41-44)
+
+
+def smooth_density(x, beta, ita):
+    """FilterOption::SmoothDensity (src/FilterOption.cpp:48-62)."""
+    if 0.0 <= x <= ita:
+        return ita * (math.exp(-beta * (1 - x / ita)) - (1 - x / ita) * math.exp(-beta))
+    if ita < x <= 1.0:
+        return (1 - ita) * (1 - math.exp(-beta * (x - ita) / (1 - ita)) + (x - ita) / (1 - ita) * math.exp(-beta)) + ita
+    raise RuntimeError("Unknown internal error")
+
+
+def smooth_density_d(x, beta, ita):
+    """PtoFderivative (src/DDAModel.cpp:340-352), as the reference writes it."""
+    if 0.0 <= x <= ita:
+        return beta * math.exp(-beta * (1 - x / ita)) + math.exp(-beta)
+    if ita < x <= 1.0:
+        return beta * math.exp(-beta * (x - ita) / (1 - ita)) + math.exp(-beta)
+    raise RuntimeError("Unknown internal error")
+
+
+class LegacyFilter:
+    """The in-plane cone filter of DDAModel::assignFreeWeightsForFilter
+    (src/DDAModel.cpp:580-712): for every free parameter i (at the first
+    dipole of its list, (xo, yo, zo)) and every parameter j, one weight
+    rfilter - dist per dipole of j in the plane z = zo within the circle
+    dist^2 <= rfilter^2 - 0.01 (circlerange / calweight, :66-77), with the
+    eight in-plane periodic images (+-Lm, +-Ln grid units) when periodic, in
+    the reference's order (own cell, (0,-1), (-1,-1), (-1,0), (-1,1), (0,1),
+    (1,1), (1,0), (1,-1)).  Quadratic in the number of parameters, as the
+    reference is: small cases only."""
+
+    def __init__(self, geometry, p2g, nfpara, rfilter, periodic, Lm, Ln, beta_min, beta_max, ita, beta_type,
+                 parameters):
+        g = np.asarray(geometry).reshape(-1, 3)
+        Lm, Ln = int(Lm), int(Ln)
+        shifts = [(0, 0)] + ([(0, -Ln), (-Lm, -Ln), (-Lm, 0), (-Lm, Ln), (0, Ln), (Lm, Ln), (Lm, 0), (Lm, -Ln)]
+                             if periodic else [])
+        r2 = rfilter * rfilter - 0.01
+        self.weights = []
+        for i in range(nfpara):
+            xo, yo, zo = (int(v) for v in g[p2g[i][0]])
+            lst = []
+            for j in range(nfpara):
+                for pos in p2g[j]:
+                    xr, yr, zr = (int(v) for v in g[pos])
+                    if zr != zo:
+                        continue
+                    for sx, sy in shifts:
+                        x, y = xr + sx, yr + sy
+                        d2 = float(x - xo) * float(x - xo) + float(y - yo) * float(y - yo)
+                        if d2 <= r2:
+                            lst.append((rfilter - math.sqrt(d2), j))
+            self.weights.append(lst)
+        self.nfpara = nfpara
+        self.beta_min, self.beta_max, self.ita, self.beta_type = beta_min, beta_max, ita, beta_type
+        self.beta = beta_min
+        self.origin = np.array(parameters, dtype=np.float64)
+        self.filtered = np.array(parameters, dtype=np.float64)
+
+    def update(self, step, it, max_it):
+        """DDAModel::UpdateStr, filter branch (src/DDAModel.cpp:785-817): the
+        raw parameters take the step (clamped to [0, 1]), are filtered and
+        projected; returns the new (physical) parameters."""
+        self.beta = beta_schedule(self.beta_type, it, max_it, self.beta_min, self.beta_max)
+        self.origin = np.clip(self.origin + np.asarray(step, dtype=np.float64), 0.0, 1.0)
+        phys = np.zeros(self.nfpara)
+        for i in range(self.nfpara):
+            num = 0.0
+            den = 0.0
+            for w, j in self.weights[i]:
+                num += w * self.origin[j]
+                den += w
+            self.filtered[i] = num / den
+            phys[i] = smooth_density(self.filtered[i], self.beta, self.ita)
+        return phys
+
+    def gradients(self, grad, it, max_it):
+        """DDAModel::gradients_filtered (src/DDAModel.cpp:354-396): each
+        parameter's gradient times the sum of its normalised weights over the
+        filters it enters, times the projection derivative at its filtered
+        value."""
+        self.beta = beta_schedule(self.beta_type, it, max_it, self.beta_min, self.beta_max)
+        res = np.zeros(self.nfpara)
+        for i in range(self.nfpara):
+            sw = 0.0
+            for w, j in self.weights[i]:
+                sw += w
+            for w, j in self.weights[i]:
+                res[j] += w / sw
+        for i in range(self.nfpara):
+            res[i] = res[i] * smooth_density_d(self.filtered[i], self.beta, self.ita) * grad[i]
+        return res

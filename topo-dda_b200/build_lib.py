@@ -17,7 +17,7 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 OUT = os.path.join(HERE, "dda_model", "libtdda.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
-SOURCES = ["lattice.cu", "operator.cu", "model.cu", "noalloc.cu", "refine.cu", "gmres.cu", "design.cu", "server.cu"]
+SOURCES = ["lattice.cu", "operator.cu", "model.cu", "noalloc.cu", "refine.cu", "gmres.cu", "design.cu", "legacy_filter.cu", "server.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",

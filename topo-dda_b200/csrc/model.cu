@@ -21,6 +21,7 @@
 #include "operator.cuh"
 #include "refine.cuh"
 #include "gmres.cuh"
+#include "legacy_filter.cuh"
 
 namespace tdda {
 
@@ -458,6 +459,8 @@ struct tdda_model {
     int obs_lo[3]{}, obs_n[3]{};
     double2 *Einc_obs = nullptr; // [nobs][3]
     double2 *Eobs = nullptr;     // [nobs][3]
+    // the reference's legacy design filter (use_filter)
+    LegacyFilter lfilter;
     // solver of later solves: 0 BiCGSTAB, 1 polynomial-preconditioned GMRES
     int solver = 0;
     GmresOptions gopt{};
@@ -770,7 +773,11 @@ tdda_status tdda_model_create(const tdda_params *p, const int32_t *geometry, con
     m->nbox = (long long)m->Nx * m->Ny * m->Nz;
     if (m->N > m->nbox) return bad("num_total exceeds num_x*num_y*num_z");
     if (p->d <= 0 || p->lam <= 0 || p->nback <= 0) return bad("d, lam and nback must be positive");
-    if (p->use_filter) return bad("useFilter=true: the legacy density filter is not part of this path");
+    if (p->use_filter) {
+        if (p->n_filters < 1 || p->filter_radii == nullptr) return bad("useFilter needs at least one filter radius");
+        if (p->is_periodic && (p->Lm != std::floor(p->Lm) || p->Ln != std::floor(p->Ln)))
+            return bad("the periodic legacy filter needs whole-cell periods Lm, Ln");
+    }
     std::string sym = p->symmetry_type ? p->symmetry_type : "";
     int dividesym;
     if (sym == "None") dividesym = 1;
@@ -855,6 +862,16 @@ tdda_status tdda_model_create(const tdda_params *p, const int32_t *geometry, con
 
     // device state
     TDDA_CUDA_TRY(cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking));
+    if (p->use_filter) {
+        // src/DDAModel.cpp:255-264: raw = filtered = the initial parameters, weights built once
+        LegacyFilterConfig fc;
+        fc.beta_min = p->beta_min; fc.beta_max = p->beta_max; fc.ita = p->ita;
+        fc.beta_type = p->beta_type ? p->beta_type : "";
+        fc.rfilter = p->filter_radii[0];
+        fc.periodic = p->is_periodic != 0;
+        fc.Lm = (int)p->Lm; fc.Ln = (int)p->Ln;
+        TRY(m->lfilter.build(fc, m->geometry, m->p2g_off, m->p2g_idx, m->parameters));
+    }
     TRY(m->op.init(m->Nx, m->Ny, m->Nz, 1));
     const ConvGeom &g = m->op.g;
     const size_t nfold = (size_t)g.hx * g.hy * g.hz * 6;
@@ -1373,6 +1390,37 @@ tdda_status tdda_set_precision(tdda_model *m, int precision) {
         return TDDA_OK;
     }
     return bad("precision must be 0 or 1");
+}
+
+tdda_status tdda_filter_update(tdda_model *m, const double *step, int64_t n, int it, int max_it) {
+    if (!m || !step) return bad("null argument");
+    if (n != m->NFpara) return bad("step must hold NFpara values");
+    std::vector<double> phys;
+    TRY(m->lfilter.update(step, it, max_it, m->stream, phys));
+    const std::vector<double> old = m->parameters;
+    const bool old_pd = m->per_dipole;
+    m->parameters = phys;
+    m->per_dipole = false;
+    tdda_status st = update_alpha(m);
+    if (st != TDDA_OK) {
+        m->parameters = old;
+        m->per_dipole = old_pd;
+    }
+    return st;
+}
+
+tdda_status tdda_filter_gradients(tdda_model *m, const double *grad, int64_t n, int it, int max_it, double *out) {
+    if (!m || !grad || !out) return bad("null argument");
+    if (n != m->NFpara) return bad("gradients must hold NFpara values");
+    return m->lfilter.gradients(grad, it, max_it, m->stream, out);
+}
+
+tdda_status tdda_filter_state(tdda_model *m, double *raw, double *filtered, int64_t n, double *beta) {
+    if (!m) return bad("null argument");
+    if (n != m->NFpara) return bad("buffers must hold NFpara values");
+    TRY(m->lfilter.state(raw, filtered, m->stream));
+    if (beta) *beta = m->lfilter.beta();
+    return TDDA_OK;
 }
 
 tdda_status tdda_set_solver(tdda_model *m, int kind, int degree, int restart) {

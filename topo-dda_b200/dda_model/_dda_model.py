@@ -91,6 +91,13 @@ class DDAModel:
         p.integral_delta = float(integralDelta)
         p.verbose = 1 if verbose else 0
         p.precision = _PRECISIONS[precision]
+        fit = np.ascontiguousarray(np.asarray(filterIterations, dtype=np.int32).ravel())
+        frad = _f64(filterRadii)
+        if fit.size != frad.size:
+            raise RuntimeError("filterIterations and filterRadii differ in length")
+        p.filter_iterations = fit.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+        p.filter_radii = _dp(frad)
+        p.n_filters = int(frad.size)
         h = ctypes.c_void_p()
         _lib.check(lib.tdda_model_create(ctypes.byref(p), geo.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
                                          _dp(diel), _dp(si), _dp(ci), si.size, ctypes.byref(h)))
@@ -285,6 +292,30 @@ class DDAModel:
         solves inside a complex128 refinement on the true residual)."""
         k = {"none": 0, "jacobi": 1}[kind]
         _lib.check(self._lib.tdda_set_preconditioner(self._handle, k))
+
+    # --- the reference's legacy filter (models created with useFilter=True) ---
+    def updateStructure(self, step, current_it, max_it):
+        """DDAModel::UpdateStr (src/DDAModel.cpp:774-838) + the polarisability
+        update: raw parameters += step (clamped), in-plane cone filter,
+        exponential projection at the scheduled beta."""
+        v = _f64(step, self.NFpara, "step")
+        _lib.check(self._lib.tdda_filter_update(self._handle, _dp(v), v.size, int(current_it), int(max_it)))
+
+    def filterGradients(self, gradients, current_it, max_it):
+        """DDAModel::gradients_filtered (src/DDAModel.cpp:354-396)."""
+        g = _f64(gradients, self.NFpara, "gradients")
+        out = np.zeros(self.NFpara)
+        _lib.check(self._lib.tdda_filter_gradients(self._handle, _dp(g), g.size, int(current_it), int(max_it),
+                                                   _dp(out)))
+        return out
+
+    def filterState(self):
+        """(raw parameters, filtered parameters, beta) of the legacy filter."""
+        raw = np.zeros(self.NFpara)
+        filt = np.zeros(self.NFpara)
+        beta = ctypes.c_double()
+        _lib.check(self._lib.tdda_filter_state(self._handle, _dp(raw), _dp(filt), raw.size, ctypes.byref(beta)))
+        return raw, filt, beta.value
 
     def setSolver(self, kind, degree=24, restart=40):
         """"bicgstab" (the reference's solver) or "pgmres": restarted GMRES on the

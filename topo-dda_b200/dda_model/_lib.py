@@ -50,6 +50,9 @@ class Params(ctypes.Structure):
         ("integral_delta", ctypes.c_double),
         ("verbose", ctypes.c_int),
         ("precision", ctypes.c_int),
+        ("filter_iterations", _ip),
+        ("filter_radii", _dp),
+        ("n_filters", ctypes.c_int),
     ]
 
 
@@ -174,6 +177,9 @@ SIGNATURES = {
     "tdda_set_precision": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "tdda_set_preconditioner": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "tdda_set_solver": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "tdda_filter_update": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_int64, ctypes.c_int, ctypes.c_int]),
+    "tdda_filter_gradients": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_int64, ctypes.c_int, ctypes.c_int, _dp]),
+    "tdda_filter_state": (ctypes.c_int, [ctypes.c_void_p, _dp, _dp, ctypes.c_int64, _dp]),
     "tdda_set_densities_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "tdda_gradient_densities_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_double,
                                                       ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(SolveInfo)]),
