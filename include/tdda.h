@@ -249,7 +249,7 @@ tdda_status tdda_set_preconditioner(tdda_model *m, int kind);
  * restarted GMRES inside complex128 iterative refinement, for systems on which
  * BiCGSTAB stalls (structures that fill their periodic cell): each refinement
  * step recomputes the true residual in complex128 and runs one GMRES cycle of
- * `restart` steps (1..256) on the Jacobi-scaled operator times a polynomial of
+ * `restart` steps (1..1024) on the Jacobi-scaled operator times a polynomial of
  * `degree` (1..64) in it, built from the harmonic Ritz values of the first
  * residual's Krylov space; inner solves in complex64 for mixed-precision
  * models.  The solve stops when ||E - A P|| / ||E|| <= tol; max_iter bounds the

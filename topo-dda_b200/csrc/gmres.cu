@@ -522,9 +522,9 @@ tdda_status pgmres_solve(const RefineWork<C> &w, GmresWork<C> &gw, const double2
             } else if (mv[k] >= max_iter || cycle == max_cycles) {
                 done[k] = 1; status[k] = TDDA_SOLVE_MAXITER;
             } else {
-                // six cycles in a row that each gain less than 1%: stagnated
-                slow[k] = (S.err > 0.99 * prev[k]) ? slow[k] + 1 : 0;
-                if (slow[k] >= 6) { done[k] = 1; status[k] = TDDA_SOLVE_STAGNATED; }
+                // twelve cycles in a row that each gain less than 0.5%: stagnated
+                slow[k] = (S.err > 0.995 * prev[k]) ? slow[k] + 1 : 0;
+                if (slow[k] >= 12) { done[k] = 1; status[k] = TDDA_SOLVE_STAGNATED; }
             }
             prev[k] = S.err;
             all &= (done[k] != 0);

@@ -1428,7 +1428,7 @@ tdda_status tdda_set_solver(tdda_model *m, int kind, int degree, int restart) {
     if (kind != 0 && kind != 1) return bad("solver must be 0 (BiCGSTAB) or 1 (polynomial-preconditioned GMRES)");
     if (kind == 1) {
         if (degree < 1 || degree > 64) return bad("polynomial degree must be in [1, 64]");
-        if (restart < 1 || restart > 256) return bad("GMRES restart must be in [1, 256]");
+        if (restart < 1 || restart > 1024) return bad("GMRES restart must be in [1, 1024]");
         m->gopt.degree = degree;
         m->gopt.restart = restart;
     }
