@@ -248,14 +248,17 @@ tdda_status tdda_set_preconditioner(tdda_model *m, int kind);
  * preconditioner setting above applies).  kind 1: polynomial-preconditioned
  * restarted GMRES inside complex128 iterative refinement, for systems on which
  * BiCGSTAB stalls (structures that fill their periodic cell): each refinement
- * step recomputes the true residual in complex128 and runs one GMRES cycle of
- * `restart` steps (1..1024) on the Jacobi-scaled operator times a polynomial of
- * `degree` (1..64) in it, built from the harmonic Ritz values of the first
- * residual's Krylov space; inner solves in complex64 for mixed-precision
- * models.  The solve stops when ||E - A P|| / ||E|| <= tol; max_iter bounds the
- * inner operator applications (tdda_solve_info: iterations = GMRES steps,
- * inner_iterations = operator applications, refinements = cycles). */
-tdda_status tdda_set_solver(tdda_model *m, int kind, int degree, int restart);
+ * step recomputes the true residual in complex128 and runs an inner solve of
+ * GMRES cycles of `restart` steps (2..1024) on the Jacobi-scaled operator times
+ * a polynomial of `degree` (1..64; 1 is plain GMRES) in it, built from the
+ * harmonic Ritz values of the first residual's Krylov space; a restart keeps
+ * the `deflate` (0..restart-1) harmonic Ritz vectors of smallest magnitude
+ * (deflated restarting, GMRES-DR).  Inner solves run in complex64 for
+ * mixed-precision models.  The solve stops when ||E - A P|| / ||E|| <= tol;
+ * max_iter bounds the inner operator applications (tdda_solve_info:
+ * iterations = GMRES steps, inner_iterations = operator applications,
+ * refinements = refinement steps). */
+tdda_status tdda_set_solver(tdda_model *m, int kind, int degree, int restart, int deflate);
 
 /* Allocation-free A.x (+ (1/alpha) o x when with_al != 0) for one vector.
  * No counterpart in the reference.  For callers that must not have device

@@ -13,13 +13,13 @@ from cases import model_args, rel
 pytestmark = pytest.mark.gpu
 
 
-def _solve(kw, precision, degree, restart, tol, B, max_iter=200000):
+def _solve(kw, precision, degree, restart, tol, B, max_iter=200000, deflate=0):
     import torch
 
     from dda_model import DDAModel
 
     m = DDAModel(**kw, precision=precision)
-    m.setSolver("pgmres", degree=degree, restart=restart)
+    m.setSolver("pgmres", degree=degree, restart=restart, deflate=deflate)
     nrhs = B.shape[0]
     Bd = torch.from_numpy(B).cuda()
     X = torch.zeros_like(Bd)
@@ -78,5 +78,27 @@ def test_pgmres_iteration_budget(sici):
     i = infos[0]
     assert i["status"] == "max_iter", i
     assert i["inner_iterations"] >= i["iterations"] * 6
-    # the polynomial's 6 steps, one cycle of 5 x 6, the correction's 6, then the budget check
-    assert 40 <= i["inner_iterations"] <= 40 + 6 * 5 + 6, i
+    # the polynomial's 6 steps, cycles of 5 x 6 checked after every step, the
+    # correction's 6, then the budget check
+    assert 40 <= i["inner_iterations"] <= 40 + 6 + 6, i
+
+
+@pytest.mark.parametrize("precision", ["complex128", "mixed"])
+@pytest.mark.parametrize("degree,restart,deflate", [(1, 16, 6), (4, 12, 4)])
+def test_deflated_restarts_match_oracle(sici, precision, degree, restart, deflate):
+    """Deflated restarting (GMRES-DR, harmonic Ritz vectors kept across
+    restarts), plain (degree 1) and with the polynomial; short cycles force
+    many restarts."""
+    from oracle.dda_oracle import OracleModel
+
+    kw = model_args(12, 12, 6, sici, MAXm=20, MAXn=20, seed=4)
+    ora = OracleModel(**kw)
+    B = _rhs(ora, 2, 8)
+    tol = 1e-8
+    X, infos = _solve(kw, precision, degree, restart, tol, B, deflate=deflate)
+    A = ora.dense_operator()
+    for k in range(2):
+        assert infos[k]["status"] == "converged", infos[k]
+        res = np.linalg.norm(B[k] - ora.aproduct_with_alb(X[k])) / np.linalg.norm(B[k])
+        assert res <= 1.0001 * tol, (k, res, infos[k])
+        assert rel(X[k], np.linalg.solve(A, B[k])) < 1e3 * tol

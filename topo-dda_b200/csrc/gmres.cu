@@ -4,6 +4,7 @@
 #include <cstring>
 #include <vector>
 
+#include "dense_eig.h"
 #include "gmres.cuh"
 
 namespace tdda {
@@ -169,40 +170,83 @@ __global__ void __launch_bounds__(kGsThreads) k_lincomb(long long n, int nv, con
     }
 }
 
+// out_l[k] = sum_{i < nin} P[k][i * ldp + l] V_i[k] for l < nout (in chunks of
+// kGsChunk outputs per CTA row): the deflated restart's new basis
+template <typename C>
+__global__ void __launch_bounds__(kGsThreads) k_lincomb_multi(long long n, int nin, int nout, const C *__restrict__ V,
+                                                              size_t vstr, size_t rstr, const double2 *__restrict__ P,
+                                                              int ldp, size_t pstr, C *__restrict__ out) {
+    pdl_wait();
+    const int k = blockIdx.z, l0 = blockIdx.y * kGsChunk;
+    const int nb = min(kGsChunk, nout - l0);
+    const C *Vk = V + (size_t)k * rstr;
+    const double2 *Pk = P + (size_t)k * pstr;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        double2 acc[kGsChunk];
+#pragma unroll
+        for (int q = 0; q < kGsChunk; ++q) acc[q] = make_double2(0.0, 0.0);
+        for (int i = 0; i < nin; ++i) {
+            const double2 b = to_d(__ldg(Vk + (size_t)i * vstr + e));
+#pragma unroll
+            for (int q = 0; q < kGsChunk; ++q)
+                if (q < nb) {
+                    const double2 c = __ldg(Pk + (size_t)i * ldp + l0 + q);
+                    acc[q].x += c.x * b.x - c.y * b.y;
+                    acc[q].y += c.x * b.y + c.y * b.x;
+                }
+        }
+#pragma unroll
+        for (int q = 0; q < kGsChunk; ++q)
+            if (q < nb) out[(size_t)(l0 + q) * vstr + (size_t)k * rstr + e] = from_d<C>(acc[q]);
+    }
+}
+
+// u += x
+template <typename C>
+__global__ void __launch_bounds__(kGsThreads) k_axpy_c(long long n, const C *__restrict__ x, C *__restrict__ u) {
+    pdl_wait();
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
+        u[e] = u[e] + x[e];
+}
+
 // ----------------------------------------------------------------------------
 // workspace
 // ----------------------------------------------------------------------------
 template <typename C> size_t GmresWork<C>::bytes() const {
     const size_t vec = sizeof(C) * (size_t)n * nrhs;
-    return vec * (restart + 3) +
-           sizeof(double2) * ((size_t)kGsBlocks * nrhs * (restart + 1) + 3 * (size_t)nrhs * (restart + 1)) +
+    return vec * (2 * (restart + 1) + 3) +
+           sizeof(double2) * ((size_t)kGsBlocks * nrhs * (restart + 1) + 3 * (size_t)nrhs * (restart + 1) +
+                              (size_t)nrhs * (restart + 1) * (deflate + 1)) +
            sizeof(double) * 2 * nrhs;
 }
 
-template <typename C> tdda_status GmresWork<C>::init(long long n3, int nrhs_, int restart_, int degree_) {
+template <typename C> tdda_status GmresWork<C>::init(long long n3, int nrhs_, int restart_, int degree_, int deflate_) {
     release();
-    n = n3; nrhs = nrhs_; restart = restart_; degree = degree_;
+    n = n3; nrhs = nrhs_; restart = restart_; degree = degree_; deflate = deflate_;
     const size_t vec = (size_t)n * nrhs;
+    C **bufs[] = {&W, &Y, &U};
+    for (C **b : bufs) TDDA_CUDA_TRY(cudaMalloc(b, sizeof(C) * vec));
     TDDA_CUDA_TRY(cudaMalloc(&V, sizeof(C) * vec * (restart + 1)));
-    TDDA_CUDA_TRY(cudaMalloc(&W, sizeof(C) * vec));
-    TDDA_CUDA_TRY(cudaMalloc(&Y, sizeof(C) * vec));
+    if (deflate > 0) TDDA_CUDA_TRY(cudaMalloc(&V2, sizeof(C) * vec * (restart + 1)));
     // cells without a dipole must read as zero in every vector
     TDDA_CUDA_TRY(cudaMemset(V, 0, sizeof(C) * vec * (restart + 1)));
-    TDDA_CUDA_TRY(cudaMemset(W, 0, sizeof(C) * vec));
-    TDDA_CUDA_TRY(cudaMemset(Y, 0, sizeof(C) * vec));
+    if (V2) TDDA_CUDA_TRY(cudaMemset(V2, 0, sizeof(C) * vec * (restart + 1)));
+    for (C **b : bufs) TDDA_CUDA_TRY(cudaMemset(*b, 0, sizeof(C) * vec));
     TDDA_CUDA_TRY(cudaMalloc(&part, sizeof(double2) * (size_t)kGsBlocks * nrhs * (restart + 1)));
     TDDA_CUDA_TRY(cudaMalloc(&h, sizeof(double2) * 2 * (size_t)nrhs * (restart + 1)));
     TDDA_CUDA_TRY(cudaMalloc(&coef, sizeof(double2) * (size_t)nrhs * (restart + 1)));
+    TDDA_CUDA_TRY(cudaMalloc(&P, sizeof(double2) * (size_t)nrhs * (restart + 1) * (deflate + 1)));
     TDDA_CUDA_TRY(cudaMalloc(&nrm, sizeof(double) * 2 * nrhs));
     TDDA_CUDA_TRY(cudaMallocHost(&h_host, sizeof(double2) * (2 * (size_t)nrhs * (restart + 1) + nrhs)));
     return TDDA_OK;
 }
 
 template <typename C> void GmresWork<C>::release() {
-    cudaFree(V); cudaFree(W); cudaFree(Y); cudaFree(part); cudaFree(h); cudaFree(coef); cudaFree(nrm);
+    cudaFree(V); cudaFree(V2); cudaFree(U); cudaFree(W); cudaFree(Y);
+    cudaFree(part); cudaFree(h); cudaFree(coef); cudaFree(P); cudaFree(nrm);
     cudaFreeHost(h_host);
-    V = W = Y = nullptr;
-    part = h = coef = nullptr;
+    V = V2 = U = W = Y = nullptr;
+    part = h = coef = P = nullptr;
     nrm = nullptr;
     h_host = nullptr;
     nrhs = 0;
@@ -417,54 +461,179 @@ tdda_status arnoldi_step(GmresWork<C> &gw, int j, OpFn op_fn, std::vector<std::v
     return TDDA_OK;
 }
 
-// Givens QR of one right-hand side's Hessenberg matrix, column by column.
-struct Givens {
+// Least-squares state of one right-hand side: the projected matrix Hbar
+// ((m+1) x m, column-major; after a deflated restart its leading block is
+// dense), its QR by Givens rotations between arbitrary row pairs, and the
+// rotated right-hand side g.
+struct LsqState {
     int m = 0;
-    std::vector<cplx> R;   // (m + 1) x m column-major, rotated
-    std::vector<cplx> c, s, g;
-    void reset(int m_, double beta) {
+    std::vector<cplx> H, R, g, c0;   // H, R: (m+1) x m; g, c0: m+1
+    struct Rot { int i, l; cplx c, s; };
+    std::vector<Rot> rots;
+    void reset(int m_) {
         m = m_;
-        R.assign((size_t)(m + 1) * m, cplx(0.0));
-        c.assign(m, cplx(0.0));
-        s.assign(m, cplx(0.0));
+        H.assign((size_t)(m + 1) * m, cplx(0.0));
+        R = H;
         g.assign(m + 1, cplx(0.0));
-        g[0] = beta;
+        c0 = g;
+        rots.clear();
     }
-    // adds column j (entries 0..j+1); returns |residual estimate|
-    double add(int j, const std::vector<cplx> &col) {
-        cplx *Rj = &R[(size_t)j * (m + 1)];
-        for (int i = 0; i <= j + 1; ++i) Rj[i] = col[i];
-        for (int i = 0; i < j; ++i) {
-            const cplx t = c[i] * Rj[i] + s[i] * Rj[i + 1];
-            Rj[i + 1] = -std::conj(s[i]) * Rj[i] + std::conj(c[i]) * Rj[i + 1];
-            Rj[i] = t;
-        }
-        const cplx a = Rj[j], b = Rj[j + 1];
-        const double den = std::sqrt(std::norm(a) + std::norm(b));
-        if (den == 0.0) {
-            c[j] = 1.0;
-            s[j] = 0.0;
-        } else {
-            c[j] = std::conj(a) / den;
-            s[j] = std::conj(b) / den;
-        }
-        Rj[j] = den;
-        Rj[j + 1] = 0.0;
-        g[j + 1] = -std::conj(s[j]) * g[j];
-        g[j] = c[j] * g[j];
-        return std::abs(g[j + 1]);
+    cplx &h(int i, int j) { return H[i + (size_t)j * (m + 1)]; }
+    cplx &r(int i, int j) { return R[i + (size_t)j * (m + 1)]; }
+    // starts from the coefficient vector c of the residual in the basis
+    void start(const std::vector<cplx> &c) {
+        std::fill(g.begin(), g.end(), cplx(0.0));
+        for (size_t i = 0; i < c.size(); ++i) g[i] = c[i];
+        c0 = g;
+        rots.clear();
     }
-    // least-squares solution of the first k columns
+    // column j of H is set (rows 0..m): rotate it into R; returns the
+    // residual estimate ||g[j+1..m]||
+    double add(int j) {
+        cplx *col = &R[(size_t)j * (m + 1)];
+        for (int i = 0; i <= m; ++i) col[i] = H[i + (size_t)j * (m + 1)];
+        for (const Rot &q : rots) {
+            const cplx a = col[q.i], b = col[q.l];
+            col[q.i] = q.c * a + q.s * b;
+            col[q.l] = -std::conj(q.s) * a + std::conj(q.c) * b;
+        }
+        for (int l = m; l > j; --l) {
+            if (col[l] == cplx(0.0)) continue;
+            const cplx a = col[j], b = col[l];
+            const double den = std::sqrt(std::norm(a) + std::norm(b));
+            Rot q{j, l, std::conj(a) / den, std::conj(b) / den};
+            col[j] = den;
+            col[l] = 0.0;
+            const cplx ga = g[j], gb = g[l];
+            g[j] = q.c * ga + q.s * gb;
+            g[l] = -std::conj(q.s) * ga + std::conj(q.c) * gb;
+            rots.push_back(q);
+        }
+        double e = 0.0;
+        for (int i = j + 1; i <= m; ++i) e += std::norm(g[i]);
+        return std::sqrt(e);
+    }
+    // least-squares solution over the first k columns
     void solve(int k, std::vector<cplx> &y) const {
         y.assign(k, cplx(0.0));
         for (int i = k - 1; i >= 0; --i) {
             cplx t = g[i];
-            for (int l = i + 1; l < k; ++l) t -= R[(size_t)l * (m + 1) + i] * y[l];
-            const cplx d = R[(size_t)i * (m + 1) + i];
+            for (int l = i + 1; l < k; ++l) t -= R[i + (size_t)l * (m + 1)] * y[l];
+            const cplx d = R[i + (size_t)i * (m + 1)];
             y[i] = d == cplx(0.0) ? cplx(0.0) : t / d;
         }
     }
 };
+
+// The deflated restart of GMRES-DR: from Hbar (k columns used, k = m), the
+// least-squares solution y and the start coefficients c0, the (m+1) x (kd+1)
+// orthonormal combination P (column-major, ld m+1) whose first kd columns
+// span the kd harmonic Ritz vectors of smallest magnitude and whose last
+// column is the residual's direction, the new projected matrix
+// P^H Hbar P[:m, :kd] ((kd+1) x kd) and the new start coefficients P^H rho.
+// Returns the number of deflation vectors kept (<= kd; 0 when the
+// eigenproblem failed: a plain restart).
+int deflated_restart(LsqState &L, int kd, const std::vector<cplx> &y, std::vector<cplx> &P,
+                     std::vector<cplx> &Hn, std::vector<cplx> &cn) {
+    const int m = L.m, ld = m + 1;
+    // residual coefficients rho = c0 - Hbar y
+    std::vector<cplx> rho(L.c0);
+    for (int j = 0; j < m; ++j)
+        for (int i = 0; i <= m; ++i) rho[i] -= L.h(i, j) * y[j];
+    std::vector<std::vector<cplx>> cols;
+    if (kd > 0) {
+        // harmonic Ritz pairs: (H_m + |h_{m+1,m}|^2 f e_m^T) g = theta g, H_m^H f = e_m
+        DenseMat Ht(m), M(m);
+        for (int i = 0; i < m; ++i)
+            for (int j = 0; j < m; ++j) {
+                Ht(i, j) = std::conj(L.h(j, i));
+                M(i, j) = L.h(i, j);
+            }
+        std::vector<cplx> f(m, cplx(0.0));
+        f[m - 1] = 1.0;
+        bool ok = dense_solve(Ht.a.data(), m, m, f.data());
+        if (ok) {
+            const double h2 = std::norm(L.h(m, m - 1));
+            for (int i = 0; i < m; ++i) M(i, m - 1) += h2 * f[i];
+            std::vector<cplx> ev;
+            ok = eigenpairs(M, ev, cols, [&](const std::vector<cplx> &e) {
+                std::vector<int> id(e.size());
+                for (size_t i = 0; i < e.size(); ++i) id[i] = (int)i;
+                std::sort(id.begin(), id.end(), [&](int a, int b) { return std::abs(e[a]) < std::abs(e[b]); });
+                id.resize(std::min<size_t>(kd, id.size()));
+                return id;
+            });
+        }
+        if (!ok) cols.clear();
+    }
+    // orthonormalise (twice), dropping dependent vectors; then the residual
+    std::vector<std::vector<cplx>> Q;
+    auto orth = [&](std::vector<cplx> v) -> bool {
+        double n0 = 0.0;
+        for (auto &e : v) n0 += std::norm(e);
+        n0 = std::sqrt(n0);
+        if (!(n0 > 0.0)) return false;
+        for (int pass = 0; pass < 2; ++pass)
+            for (auto &q : Q) {
+                cplx d = 0.0;
+                for (int i = 0; i <= m; ++i) d += std::conj(q[i]) * v[i];
+                for (int i = 0; i <= m; ++i) v[i] -= d * q[i];
+            }
+        double n1 = 0.0;
+        for (auto &e : v) n1 += std::norm(e);
+        n1 = std::sqrt(n1);
+        if (!(n1 > 1e-8 * n0)) return false;
+        for (auto &e : v) e /= n1;
+        Q.push_back(v);
+        return true;
+    };
+    for (auto &c : cols) {
+        std::vector<cplx> v(m + 1, cplx(0.0));
+        for (int i = 0; i < m; ++i) v[i] = c[i];
+        orth(v);
+    }
+    const int kept = (int)Q.size();
+    if (!orth(rho)) {
+        // the residual lies in the deflation space: keep its plain direction
+        Q.clear();
+        Q.push_back(rho);
+        double nr = 0.0;
+        for (auto &e : Q[0]) nr += std::norm(e);
+        nr = std::sqrt(nr);
+        for (auto &e : Q[0]) e = nr > 0 ? e / nr : cplx(0.0);
+        P.assign(ld, cplx(0.0));
+        for (int i = 0; i <= m; ++i) P[i] = Q[0][i];
+        Hn.clear();
+        cn.assign(1, cplx(nr, 0.0));
+        return 0;
+    }
+    const int nc = kept + 1;
+    P.assign((size_t)ld * nc, cplx(0.0));
+    for (int c = 0; c < nc; ++c)
+        for (int i = 0; i <= m; ++i) P[i + (size_t)c * ld] = Q[c][i];
+    // Hn = P^H Hbar P[:m, :kept]  ((kept+1) x kept)
+    std::vector<cplx> HP((size_t)ld * kept, cplx(0.0));
+    for (int c = 0; c < kept; ++c)
+        for (int j = 0; j < m; ++j) {
+            const cplx pj = P[j + (size_t)c * ld];
+            if (pj == cplx(0.0)) continue;
+            for (int i = 0; i <= m; ++i) HP[i + (size_t)c * ld] += L.h(i, j) * pj;
+        }
+    Hn.assign((size_t)nc * kept, cplx(0.0));
+    for (int c = 0; c < kept; ++c)
+        for (int r = 0; r < nc; ++r) {
+            cplx s = 0.0;
+            for (int i = 0; i <= m; ++i) s += std::conj(P[i + (size_t)r * ld]) * HP[i + (size_t)c * ld];
+            Hn[r + (size_t)c * nc] = s;
+        }
+    cn.assign(nc, cplx(0.0));
+    for (int r = 0; r < nc; ++r) {
+        cplx s = 0.0;
+        for (int i = 0; i <= m; ++i) s += std::conj(P[i + (size_t)r * ld]) * rho[i];
+        cn[r] = s;
+    }
+    return kept;
+}
 
 }  // namespace
 
@@ -473,18 +642,22 @@ tdda_status pgmres_solve(const RefineWork<C> &w, GmresWork<C> &gw, const double2
                          bool x0_zero, int max_iter, double tol, const GmresOptions &o, tdda_solve_info *info) {
     const long long n = 3 * w.nbox;
     cudaStream_t s = w.s;
-    if (gw.nrhs != nrhs || gw.n != n || gw.restart != o.restart || gw.degree != o.degree) {
+    if (gw.nrhs != nrhs || gw.n != n || gw.restart != o.restart || gw.degree != o.degree || gw.deflate != o.deflate) {
         set_error("GMRES workspace does not match the solve");
         return TDDA_ERR_STATE;
     }
+    if (o.deflate >= o.restart) {
+        set_error("GMRES: the deflation vectors must be fewer than the restart length");
+        return TDDA_ERR_BAD_ARG;
+    }
     if (x0_zero) TDDA_CUDA_TRY(cudaMemsetAsync(X, 0, sizeof(double2) * n * nrhs, s));
-    const int m = o.restart, d = o.degree;
-    std::vector<int> done(nrhs, 0), cycles(nrhs, 0), steps(nrhs, 0), status(nrhs, TDDA_SOLVE_RUNNING), slow(nrhs, 0);
+    const int m = o.restart, d = o.degree, ld = m + 1;
+    std::vector<int> done(nrhs, 0), refines(nrhs, 0), steps(nrhs, 0), status(nrhs, TDDA_SOLVE_RUNNING), slow(nrhs, 0);
     std::vector<long long> mv(nrhs, 0);
-    std::vector<double> err(nrhs, 0.0), prev(nrhs, 1e300), beta(nrhs, 0.0);
+    std::vector<double> err(nrhs, 0.0), prev(nrhs, 1e300);
     std::vector<cplx> roots;
     std::vector<std::vector<cplx>> Hcol(nrhs);
-    std::vector<Givens> qr(nrhs);
+    std::vector<LsqState> L(nrhs);
     double *h = w.h_part;
     // the inner operator, and the inner operator times the polynomial
     auto op_plain = [&](const C *x, C *y) { return apply_scaled<C>(*w.op, w.sc, w.al, x, y, nrhs, w.dstride, s); };
@@ -501,8 +674,9 @@ tdda_status pgmres_solve(const RefineWork<C> &w, GmresWork<C> &gw, const double2
         }
         return TDDA_OK;
     };
-    const int max_cycles = 100000;
-    for (int cycle = 0; cycle <= max_cycles; ++cycle) {
+    const size_t vstr = (size_t)n * nrhs;
+    const int max_refine = 60;
+    for (int outer = 0; outer <= max_refine; ++outer) {
         tdda_status st = residual_c128(*w.op64, w.al64, B, X, w.Rm, w.st_res, nrhs, s, w.dstride);
         if (st != TDDA_OK) return st;
         TDDA_CUDA_TRY(cudaMemcpyAsync(w.st_res_host, w.st_res, sizeof(SolverState) * nrhs, cudaMemcpyDeviceToHost, s));
@@ -519,12 +693,12 @@ tdda_status pgmres_solve(const RefineWork<C> &w, GmresWork<C> &gw, const double2
                 done[k] = 1; status[k] = TDDA_SOLVE_CONVERGED;
             } else if (!std::isfinite(S.err)) {
                 done[k] = 1; status[k] = TDDA_SOLVE_NONFINITE;
-            } else if (mv[k] >= max_iter || cycle == max_cycles) {
+            } else if (mv[k] >= max_iter || outer == max_refine) {
                 done[k] = 1; status[k] = TDDA_SOLVE_MAXITER;
             } else {
-                // twelve cycles in a row that each gain less than 0.5%: stagnated
-                slow[k] = (S.err > 0.995 * prev[k]) ? slow[k] + 1 : 0;
-                if (slow[k] >= 12) { done[k] = 1; status[k] = TDDA_SOLVE_STAGNATED; }
+                // two refinements in a row that do not halve the true residual: stagnated
+                slow[k] = (S.err > 0.5 * prev[k]) ? slow[k] + 1 : 0;
+                if (slow[k] >= 2) { done[k] = 1; status[k] = TDDA_SOLVE_STAGNATED; }
             }
             prev[k] = S.err;
             all &= (done[k] != 0);
@@ -538,15 +712,17 @@ tdda_status pgmres_solve(const RefineWork<C> &w, GmresWork<C> &gw, const double2
             const double rn = S.err * S.enorm;
             h[k] = 1.0 / rn;
             h[nrhs + k] = rn;
-            h[2 * nrhs + k] = std::max(0.5 * tol / S.err, o.floor);  // reduction this cycle must reach
+            h[2 * nrhs + k] = std::max(0.5 * tol / S.err, o.floor);  // reduction this inner solve must reach
         }
         TDDA_CUDA_TRY(cudaMemcpyAsync(w.d_part, h, sizeof(double) * 3 * nrhs, cudaMemcpyHostToDevice, s));
         launch_to_inner<C>(n, w.nbox, nrhs, w.dstride, w.Rm, w.d_part, w.sc64, w.R, s);
-        // V[0] = R^ / ||R^||
-        gs_update(gw, 0, gw.h, 0, w.R, true, s);  // norms only (no basis vectors)
+        // V[0] = R^ / ||R^||, U = 0
+        gs_update(gw, 0, gw.h, 0, w.R, true, s);  // norms only
         scale_vec(gw, gw.nrm + nrhs, w.R, basis(gw, 0), s);
+        TDDA_CUDA_TRY(cudaMemsetAsync(gw.U, 0, sizeof(C) * vstr, s));
         TDDA_CUDA_TRY(cudaMemcpyAsync(gw.h_host, gw.nrm, sizeof(double) * nrhs, cudaMemcpyDeviceToHost, s));
         TDDA_CUDA_TRY(cudaStreamSynchronize(s));
+        std::vector<double> beta(nrhs);
         for (int k = 0; k < nrhs; ++k) beta[k] = reinterpret_cast<const double *>(gw.h_host)[k];
         if (roots.empty()) {
             // the polynomial: Arnoldi steps of the inner operator on the first
@@ -577,46 +753,137 @@ tdda_status pgmres_solve(const RefineWork<C> &w, GmresWork<C> &gw, const double2
                 }
             leja_order(th);
             roots = th;
-            // V[0] is unchanged by those steps; the cycle overwrites V[1..]
+            // V[0] is unchanged by those steps; the cycles overwrite V[1..]
         }
-        // one GMRES cycle on Ah p(Ah)
-        for (int k = 0; k < nrhs; ++k) qr[k].reset(m, beta[k]);
-        int kk = 0;
-        for (int j = 0; j < m; ++j) {
-            st = arnoldi_step(gw, j, op_poly, Hcol, s);
-            if (st != TDDA_OK) return st;
-            kk = j + 1;
-            bool reached = true;
-            for (int k = 0; k < nrhs; ++k) {
-                if (done[k]) continue;
-                const double est = qr[k].add(j, Hcol[k]);
-                mv[k] += (long long)roots.size();
-                steps[k] += 1;
-                if (!(est <= h[2 * nrhs + k] * beta[k]) && mv[k] < max_iter) reached = false;
-            }
-            if (reached) break;
-        }
-        // correction u = V y, D = p(Ah) u, X += ||R|| S D
-        std::vector<double2> coef((size_t)nrhs * kk, make_double2(0.0, 0.0));
+        // the inner solve: (deflated) restarted GMRES cycles on Ah p(Ah)
         for (int k = 0; k < nrhs; ++k) {
-            if (done[k]) continue;
-            std::vector<cplx> y;
-            qr[k].solve(kk, y);
-            for (int i = 0; i < kk; ++i) coef[(size_t)k * kk + i] = make_double2(y[i].real(), y[i].imag());
-            cycles[k] += 1;
+            L[k].reset(m);
+            L[k].start({cplx(beta[k], 0.0)});
         }
-        TDDA_CUDA_TRY(cudaMemcpyAsync(gw.coef, coef.data(), sizeof(double2) * coef.size(), cudaMemcpyHostToDevice, s));
-        count_launches(1);
-        launch_dep(k_lincomb<C>, dim3(gs_blocks(n), 1, nrhs), dim3(kGsThreads), sizeof(double2) * kk, s, n, kk,
-                   (const C *)gw.V, (size_t)n * nrhs, (size_t)n, (const double2 *)gw.coef, kk, w.D);
+        int kd = 0;                      // deflation vectors at the start of this cycle
+        std::vector<double> cyc_prev(beta);
+        std::vector<int> inner_slow(nrhs, 0), inner_done(nrhs, 0);
+        for (int k = 0; k < nrhs; ++k) inner_done[k] = done[k];
+        for (int cycle = 0;; ++cycle) {
+            int jc = kd;                 // columns of Hbar filled
+            for (int k = 0; k < nrhs; ++k)
+                if (!inner_done[k])
+                    for (int j = 0; j < kd; ++j) L[k].add(j);
+            bool reached = false;
+            for (int j = kd; j < m; ++j) {
+                st = arnoldi_step(gw, j, op_poly, Hcol, s);
+                if (st != TDDA_OK) return st;
+                jc = j + 1;
+                reached = true;
+                for (int k = 0; k < nrhs; ++k) {
+                    if (inner_done[k]) continue;
+                    for (int i = 0; i <= j + 1; ++i) L[k].h(i, j) = Hcol[k][i];
+                    const double est = L[k].add(j);
+                    mv[k] += (long long)roots.size();
+                    steps[k] += 1;
+                    if (!(est <= h[2 * nrhs + k] * beta[k]) && mv[k] < max_iter) reached = false;
+                }
+                if (reached) break;
+            }
+            // u += V y over the jc columns
+            std::vector<double2> coef((size_t)nrhs * jc, make_double2(0.0, 0.0));
+            std::vector<std::vector<cplx>> ys(nrhs);
+            bool all_in = true;
+            for (int k = 0; k < nrhs; ++k) {
+                if (inner_done[k]) continue;
+                L[k].solve(jc, ys[k]);
+                for (int i = 0; i < jc; ++i) coef[(size_t)k * jc + i] = make_double2(ys[k][i].real(), ys[k][i].imag());
+                double est = 0.0;
+                for (int i = jc; i <= m; ++i) est += std::norm(L[k].g[i]);
+                est = std::sqrt(est);
+                // twelve cycles in a row that each gain less than 0.5%: the inner
+                // solve has given what it can; the refinement takes over
+                inner_slow[k] = (est > 0.995 * cyc_prev[k]) ? inner_slow[k] + 1 : 0;
+                cyc_prev[k] = est;
+                if (est <= h[2 * nrhs + k] * beta[k] || mv[k] >= max_iter || inner_slow[k] >= 12) inner_done[k] = 1;
+                all_in &= (inner_done[k] != 0);
+            }
+            TDDA_CUDA_TRY(cudaMemcpyAsync(gw.coef, coef.data(), sizeof(double2) * coef.size(), cudaMemcpyHostToDevice, s));
+            count_launches(1);
+            launch_dep(k_lincomb<C>, dim3(gs_blocks(n), 1, nrhs), dim3(kGsThreads), sizeof(double2) * jc, s, n, jc,
+                       (const C *)gw.V, vstr, (size_t)n, (const double2 *)gw.coef, jc, gw.W);
+            // U += W (the combination lands in W first: k_lincomb overwrites)
+            count_launches(1);
+            launch_dep(k_axpy_c<C>, dim3(gs_blocks(n * nrhs)), dim3(kGsThreads), 0, s, n * nrhs, (const C *)gw.W, gw.U);
+            if (all_in || cycle > 100000) break;
+            // restart: deflated (GMRES-DR) or plain from the current residual
+            std::vector<std::vector<cplx>> Ps(nrhs), Hns(nrhs), cns(nrhs);
+            int kept = o.deflate;
+            for (int k = 0; k < nrhs; ++k) {
+                if (inner_done[k]) continue;
+                std::vector<cplx> yfull(m, cplx(0.0));
+                for (int i = 0; i < jc; ++i) yfull[i] = ys[k][i];
+                kept = std::min(kept, deflated_restart(L[k], o.deflate, yfull, Ps[k], Hns[k], cns[k]));
+            }
+            // every right-hand side keeps the same number of vectors
+            for (int k = 0; k < nrhs; ++k) {
+                if (inner_done[k]) continue;
+                const int have = (int)(Ps[k].size() / ld) - 1;
+                if (have != kept) {
+                    std::vector<cplx> yfull(m, cplx(0.0));
+                    for (int i = 0; i < jc; ++i) yfull[i] = ys[k][i];
+                    deflated_restart(L[k], kept, yfull, Ps[k], Hns[k], cns[k]);
+                    if ((int)(Ps[k].size() / ld) - 1 != kept) kept = 0;
+                }
+            }
+            if (kept == 0)
+                for (int k = 0; k < nrhs; ++k) {
+                    if (inner_done[k]) continue;
+                    std::vector<cplx> yfull(m, cplx(0.0));
+                    for (int i = 0; i < jc; ++i) yfull[i] = ys[k][i];
+                    deflated_restart(L[k], 0, yfull, Ps[k], Hns[k], cns[k]);
+                }
+            const int nc = kept + 1;
+            std::vector<double2> Pd((size_t)nrhs * ld * nc, make_double2(0.0, 0.0));
+            for (int k = 0; k < nrhs; ++k) {
+                if (inner_done[k]) continue;
+                for (int i = 0; i <= m; ++i)
+                    for (int c = 0; c < nc; ++c) {
+                        const cplx v = Ps[k][i + (size_t)c * ld];
+                        Pd[(size_t)k * ld * nc + (size_t)i * nc + c] = make_double2(v.real(), v.imag());
+                    }
+            }
+            TDDA_CUDA_TRY(cudaMemcpyAsync(gw.P, Pd.data(), sizeof(double2) * Pd.size(), cudaMemcpyHostToDevice, s));
+            if (nc == 1) {
+                // plain restart: V[0] = V P in place of a second basis
+                count_launches(1);
+                launch_dep(k_lincomb_multi<C>, dim3(gs_blocks(n), 1, nrhs), dim3(kGsThreads), 0, s, n, m + 1, 1,
+                           (const C *)gw.V, vstr, (size_t)n, (const double2 *)gw.P, 1, (size_t)ld, gw.W);
+                TDDA_CUDA_TRY(cudaMemcpyAsync(gw.V, gw.W, sizeof(C) * vstr, cudaMemcpyDeviceToDevice, s));
+            } else {
+                count_launches(1);
+                launch_dep(k_lincomb_multi<C>, dim3(gs_blocks(n), (nc + kGsChunk - 1) / kGsChunk, nrhs),
+                           dim3(kGsThreads), 0, s, n, m + 1, nc, (const C *)gw.V, vstr, (size_t)n,
+                           (const double2 *)gw.P, nc, (size_t)ld * nc, gw.V2);
+                std::swap(gw.V, gw.V2);
+            }
+            TDDA_CUDA_TRY(cudaGetLastError());
+            for (int k = 0; k < nrhs; ++k) {
+                if (inner_done[k]) continue;
+                L[k].reset(m);
+                for (int c = 0; c < kept; ++c)
+                    for (int r = 0; r < nc; ++r) L[k].h(r, c) = Hns[k][r + (size_t)c * nc];
+                L[k].start(cns[k]);
+            }
+            kd = kept;
+        }
+        // correction D = p(Ah) U, X += ||R|| S D
         for (int i = 0; i < (int)roots.size(); ++i) {
             const cplx c = 1.0 / roots[i];
-            st = poly_factor<C>(*w.op, w.sc, w.al, i == 0 ? w.D : gw.W, gw.W, gw.Y, i == 0, nullptr, nullptr,
+            st = poly_factor<C>(*w.op, w.sc, w.al, i == 0 ? gw.U : gw.W, gw.W, gw.Y, i == 0, nullptr, nullptr,
                                 make_double2(c.real(), c.imag()), nrhs, w.dstride, s);
             if (st != TDDA_OK) return st;
         }
         for (int k = 0; k < nrhs; ++k)
-            if (!done[k]) mv[k] += (long long)roots.size();
+            if (!done[k]) {
+                mv[k] += (long long)roots.size();
+                refines[k] += 1;
+            }
         launch_axpy_inner<C>(n, w.nbox, nrhs, w.dstride, w.d_part + nrhs, w.sc64, gw.Y, X, s);
         TDDA_CUDA_TRY(cudaGetLastError());
     }
@@ -625,7 +892,7 @@ tdda_status pgmres_solve(const RefineWork<C> &w, GmresWork<C> &gw, const double2
             info[k].iterations = steps[k];
             info[k].error = err[k];
             info[k].status = status[k];
-            info[k].refinements = cycles[k];
+            info[k].refinements = refines[k];
             info[k].inner_iterations = (int)std::min<long long>(mv[k], 2147483647LL);
             info[k].true_error = err[k];
         }

@@ -29,16 +29,18 @@ using cplx = std::complex<double>;
 
 // Device vectors of one polynomial-preconditioned GMRES instance.
 template <typename C> struct GmresWork {
-    int restart = 0, degree = 0, nrhs = 0;
+    int restart = 0, degree = 0, deflate = 0, nrhs = 0;
     long long n = 0;            // 3 * nbox
-    C *V = nullptr;             // basis [restart + 1][nrhs][n]
+    C *V = nullptr, *V2 = nullptr;  // basis and the deflated restart's new basis [restart + 1][nrhs][n]
+    C *U = nullptr;             // inner solution accumulated over cycles [nrhs][n]
     C *W = nullptr, *Y = nullptr;  // polynomial work vector and accumulator [nrhs][n]
     double2 *part = nullptr;    // block partial sums
     double2 *h = nullptr;       // device sums [2][nrhs][restart + 1]
     double *nrm = nullptr;      // device norms / reciprocals [2][nrhs]
     double2 *coef = nullptr;    // device [nrhs][restart + 1] combination weights
+    double2 *P = nullptr;       // device [nrhs][restart + 1][deflate + 1] restart combinations
     double2 *h_host = nullptr;  // pinned mirror of h, nrm
-    tdda_status init(long long n3, int nrhs, int restart, int degree);
+    tdda_status init(long long n3, int nrhs, int restart, int degree, int deflate);
     void release();
     size_t bytes() const;
 };
@@ -46,15 +48,19 @@ template <typename C> struct GmresWork {
 // Options of the solver.
 struct GmresOptions {
     int degree = 24;        // polynomial degree (operator applications per preconditioned step)
-    int restart = 40;       // GMRES steps per cycle (one cycle per refinement step)
-    double floor = 0.0;     // do not ask a cycle for a relative reduction below this
+    int restart = 40;       // GMRES steps per cycle
+    int deflate = 0;        // harmonic Ritz vectors kept across restarts (GMRES-DR), < restart
+    double floor = 0.0;     // an inner solve stops once it has cut its residual by this much
 };
 
 // Solves (A + diag al) X = B to a TRUE relative residual <= tol per
 // right-hand side (w: the refinement workspace of the inner precision C).
-// info[k].iterations = preconditioned GMRES steps, inner_iterations = inner
-// operator applications, refinements = cycles.  max_iter bounds the inner
-// operator applications.
+// Each refinement step recomputes the true residual R in complex128 and runs
+// an inner solve of (deflated) restarted GMRES cycles on the scaled operator
+// times the polynomial until the inner residual has dropped by
+// max(tol / (2 ||R||/||B||), floor).  info[k].iterations = GMRES steps,
+// inner_iterations = inner operator applications, refinements = refinement
+// steps.  max_iter bounds the inner operator applications.
 template <typename C>
 tdda_status pgmres_solve(const RefineWork<C> &w, GmresWork<C> &gw, const double2 *B, double2 *X, int nrhs,
                          bool x0_zero, int max_iter, double tol, const GmresOptions &o, tdda_solve_info *info);

@@ -707,9 +707,10 @@ static tdda_status solve_pgmres(tdda_model *m, const double2 *B, double2 *X, int
                                 double tol, tdda_solve_info *info) {
     TRY(ensure_refine(m, nrhs, (C *)nullptr));
     GmresWork<C> &gw = gmres_work(m, (C *)nullptr);
-    if (gw.nrhs != nrhs || gw.restart != m->gopt.restart || gw.degree != m->gopt.degree) {
+    if (gw.nrhs != nrhs || gw.restart != m->gopt.restart || gw.degree != m->gopt.degree ||
+        gw.deflate != m->gopt.deflate) {
         gw.release();
-        TRY(gw.init(3 * m->nbox, nrhs, m->gopt.restart, m->gopt.degree));
+        TRY(gw.init(3 * m->nbox, nrhs, m->gopt.restart, m->gopt.degree, m->gopt.deflate));
     }
     const int saved = m->precond;
     m->precond = 1;
@@ -1423,14 +1424,16 @@ tdda_status tdda_filter_state(tdda_model *m, double *raw, double *filtered, int6
     return TDDA_OK;
 }
 
-tdda_status tdda_set_solver(tdda_model *m, int kind, int degree, int restart) {
+tdda_status tdda_set_solver(tdda_model *m, int kind, int degree, int restart, int deflate) {
     if (m == nullptr) return bad("null model");
     if (kind != 0 && kind != 1) return bad("solver must be 0 (BiCGSTAB) or 1 (polynomial-preconditioned GMRES)");
     if (kind == 1) {
         if (degree < 1 || degree > 64) return bad("polynomial degree must be in [1, 64]");
-        if (restart < 1 || restart > 1024) return bad("GMRES restart must be in [1, 1024]");
+        if (restart < 2 || restart > 1024) return bad("GMRES restart must be in [2, 1024]");
+        if (deflate < 0 || deflate >= restart) return bad("deflation vectors must be in [0, restart)");
         m->gopt.degree = degree;
         m->gopt.restart = restart;
+        m->gopt.deflate = deflate;
     }
     m->solver = kind;
     return TDDA_OK;

@@ -317,13 +317,14 @@ class DDAModel:
         _lib.check(self._lib.tdda_filter_state(self._handle, _dp(raw), _dp(filt), raw.size, ctypes.byref(beta)))
         return raw, filt, beta.value
 
-    def setSolver(self, kind, degree=24, restart=40):
+    def setSolver(self, kind, degree=24, restart=40, deflate=0):
         """"bicgstab" (the reference's solver) or "pgmres": restarted GMRES on the
-        Jacobi-scaled operator times a polynomial of `degree` in it, one cycle of
-        `restart` steps per complex128 refinement step (for structures that fill
-        their periodic cell, where BiCGSTAB stalls)."""
+        Jacobi-scaled operator times a polynomial of `degree` in it, cycles of
+        `restart` steps keeping `deflate` harmonic Ritz vectors across restarts,
+        inside complex128 refinement (for structures that fill their periodic
+        cell, where BiCGSTAB stalls)."""
         k = {"bicgstab": 0, "pgmres": 1}[kind]
-        _lib.check(self._lib.tdda_set_solver(self._handle, k, int(degree), int(restart)))
+        _lib.check(self._lib.tdda_set_solver(self._handle, k, int(degree), int(restart), int(deflate)))
 
     @staticmethod
     def kernel_launches():

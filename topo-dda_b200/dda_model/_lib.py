@@ -176,7 +176,7 @@ SIGNATURES = {
     "tdda_lattice_offsets_device": (ctypes.c_int, [ctypes.c_void_p, _ip, _ip, ctypes.c_void_p, ctypes.c_void_p]),
     "tdda_set_precision": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "tdda_set_preconditioner": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
-    "tdda_set_solver": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "tdda_set_solver": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "tdda_filter_update": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_int64, ctypes.c_int, ctypes.c_int]),
     "tdda_filter_gradients": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_int64, ctypes.c_int, ctypes.c_int, _dp]),
     "tdda_filter_state": (ctypes.c_int, [ctypes.c_void_p, _dp, _dp, ctypes.c_int64, _dp]),
