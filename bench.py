@@ -326,6 +326,49 @@ def run_reference(args):
     return 0
 
 
+def cpu_lattice_rate(w, npts=200, seed=3):
+    """Image evaluations per second of the oracle's restatement of the
+    reference's constructor loop (src/AProductCore.cpp:63-244: every padded
+    offset sums every image (m, n), |m|,|n| <= M, damped; single thread, as the
+    reference's constructor), timed on npts random offsets of the grid."""
+    import ctypes
+
+    from oracle import dda_oracle as O
+
+    lib = O._load_lib()
+    si, ci = O.sici_tables()
+    rng = np.random.default_rng(seed)
+    d = w["d"]
+    off = np.stack([rng.integers(-(w[a] - 1), w[a], npts) for a in ("nx", "ny", "nz")], axis=1).astype(np.float64) * d
+    off = np.ascontiguousarray(off)
+    out = np.zeros(12 * npts)
+    K = 2 * math.pi / w["lam"]
+    dp = ctypes.POINTER(ctypes.c_double)
+    t0 = time.perf_counter()
+    lib.oracle_lattice_points(0, npts, off.ctypes.data_as(dp), w["M"], w["M"], w["period"] * d, w["period"] * d, K, d,
+                              si.ctypes.data_as(dp), ci.ctypes.data_as(dp), len(si), 0.1, out.ctypes.data_as(dp))
+    dt = time.perf_counter() - t0
+    return npts * (2 * w["M"] + 1) ** 2 / dt, dt
+
+
+def lattice_record(m, w, cpu_rate=None):
+    """The lattice-sum kernel of one model: device time, and the work the
+    reference's constructor does for the same tensor ((2nx-1)(2ny-1)(2nz-1)
+    offsets x (2M+1)^2 images) per second of it."""
+    nfft = (2 * w["nx"] - 1) * (2 * w["ny"] - 1) * (2 * w["nz"] - 1)
+    evals = nfft * (2 * w["M"] + 1) ** 2
+    ms = m.info["lattice_ms"]
+    rec = {"lattice_ms": ms, "tensor_fft_ms": m.info["tensor_fft_ms"], "reference_image_evaluations": evals,
+           "reference_equivalent_evals_per_s": evals / (ms * 1e-3),
+           "note": "the kernel evaluates the non-negative octant (parity gives the rest) and skips images whose "
+                   "damping exp(-(0.01 K r)^4) is exactly 0; FP64-issue-bound, not graded against HBM"}
+    if cpu_rate is not None:
+        rec["cpu_port_evals_per_s_1_thread"] = cpu_rate
+        rec["cpu_port_constructor_estimate_s"] = evals / cpu_rate
+        rec["speedup_vs_cpu_constructor"] = (evals / cpu_rate) / (ms * 1e-3)
+    return rec
+
+
 def config_block(w, ngpu):
     per = f"periodic {w['period']}d, |m|,|n|<={w['M']}" if w["M"] > 0 else "isolated (no periodic images)"
     return {"workload": f"{w['nx']}x{w['ny']}x{w['nz']} dipoles, {per}, d=25nm, lambda=542nm, eps 3.5+0.01i, "
