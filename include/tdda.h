@@ -39,7 +39,8 @@ typedef enum {
     TDDA_SOLVE_BREAKDOWN = 3,   /* r0 . rl == 0 (src/DDAModel.cpp:952-970) */
     TDDA_SOLVE_NONFINITE = 4,   /* residual became NaN/Inf */
     TDDA_SOLVE_ZERO_RHS = 5,    /* ||E|| == 0: solution is 0 */
-    TDDA_SOLVE_STAGNATED = 6    /* mixed precision: residual stopped decreasing */
+    TDDA_SOLVE_STAGNATED = 6,   /* mixed precision: residual stopped decreasing */
+    TDDA_SOLVE_TIMEOUT = 7      /* the device-side time limit of the solve ran out */
 } tdda_solve_status;
 
 typedef enum { TDDA_PREC_C128 = 0, TDDA_PREC_MIXED = 1 } tdda_precision;
@@ -242,6 +243,14 @@ tdda_status tdda_set_precision(tdda_model *m, int precision);
  * inside a complex128 iterative refinement that stops on the true residual
  * (the default for mixed-precision models). */
 tdda_status tdda_set_preconditioner(tdda_model *m, int kind);
+
+/* Device-side time limit of later BiCGSTAB solves, in seconds (0: none; no
+ * reference counterpart).  BiCGSTAB iterations run as one CUDA graph launch
+ * whose while-node repeats them on the device until every right-hand side is
+ * done; the loop ends right-hand sides still running after this long with
+ * status TDDA_SOLVE_TIMEOUT, and after max_iter iterations with
+ * TDDA_SOLVE_MAXITER, without any host poll. */
+tdda_status tdda_set_time_limit(tdda_model *m, double seconds);
 
 /* Solver of later solves (no reference counterpart; the reference always runs
  * BiCGSTAB, src/DDAModel.cpp:899-1009).  kind 0: BiCGSTAB (default; the

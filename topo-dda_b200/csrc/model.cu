@@ -461,6 +461,7 @@ struct tdda_model {
     double2 *Eobs = nullptr;     // [nobs][3]
     // the reference's legacy design filter (use_filter)
     LegacyFilter lfilter;
+    double time_limit_s = 0.0;             // device-side time limit of BiCGSTAB solves
     // solver of later solves: 0 BiCGSTAB, 1 polynomial-preconditioned GMRES
     int solver = 0;
     GmresOptions gopt{};
@@ -662,6 +663,7 @@ static tdda_status solve_c128(tdda_model *m, const double2 *B, double2 *X, int n
     TRY(ensure_krylov(m, nrhs));
     KrylovOptions o;
     o.graph_steps = kGraphSteps;
+    o.time_limit_s = m->time_limit_s;
     return bicgstab_device<double2>(m->op, m->kv, m->al, nullptr, B, X, nrhs, x0_zero, max_iter, tol, m->stream,
                                     info, o);
 }
@@ -693,7 +695,7 @@ static tdda_status solve_refined(tdda_model *m, const double2 *B, double2 *X, in
     w.op64 = &m->op; w.al64 = m->al; w.sc64 = m->precond ? m->sc64 : nullptr;
     w.Rm = m->Rm; w.st_res = m->st_res; w.st_res_host = m->st_res_host;
     w.d_part = m->d_part; w.h_part = m->h_part;
-    w.nbox = m->nbox; w.s = m->stream; w.graph_steps = kGraphSteps;
+    w.nbox = m->nbox; w.s = m->stream; w.graph_steps = kGraphSteps; w.time_limit_s = m->time_limit_s;
     return refine_solve<C>(w, B, X, nrhs, x0_zero, max_iter, tol, info);
 }
 
@@ -1391,6 +1393,13 @@ tdda_status tdda_set_precision(tdda_model *m, int precision) {
         return TDDA_OK;
     }
     return bad("precision must be 0 or 1");
+}
+
+tdda_status tdda_set_time_limit(tdda_model *m, double seconds) {
+    if (m == nullptr) return bad("null model");
+    if (!(seconds >= 0.0)) return bad("time limit must be >= 0");
+    m->time_limit_s = seconds;
+    return TDDA_OK;
 }
 
 tdda_status tdda_filter_update(tdda_model *m, const double *step, int64_t n, int it, int max_it) {

@@ -1092,6 +1092,47 @@ __global__ void __launch_bounds__(NT) k_init_zero(long long n, const C *__restri
     reduce_finalize<2>(acc, part + (size_t)rhs * pstride, counter + rhs, blockIdx.x, gridDim.x, fin, rhs);
 }
 
+// The device-driven iteration loop (a CUDA graph whose while-node repeats the
+// BiCGSTAB iterations): the start kernel zeroes the pass counter and records
+// the start time; the condition kernel, last in the loop body, keeps the loop
+// going while some right-hand side runs.  Past `cap` passes or `limit_ns`
+// nanoseconds the running right-hand sides end (MAXITER / TIMEOUT), so the
+// loop ends after at most `cap` passes whatever the states hold.
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__global__ void k_loop_start(unsigned long long *loop) {
+    if (threadIdx.x == 0) {
+        loop[0] = 0;
+        loop[1] = global_ns();
+    }
+}
+
+__global__ void k_loop_cond(cudaGraphConditionalHandle h, SolverState *st, int nrhs, unsigned long long *loop,
+                            unsigned long long cap, unsigned long long limit_ns) {
+    if (threadIdx.x != 0) return;
+    const unsigned long long c = ++loop[0];
+    const bool over_time = limit_ns > 0 && global_ns() - loop[1] > limit_ns;
+    const bool over_cap = c >= cap;
+    int running = 0;
+    for (int k = 0; k < nrhs; ++k) {
+        if (st[k].done) continue;
+        if (over_time) {
+            st[k].done = 1;
+            st[k].status = TDDA_SOLVE_TIMEOUT;
+        } else if (over_cap) {
+            st[k].done = 1;
+            st[k].status = TDDA_SOLVE_MAXITER;
+        } else {
+            running = 1;
+        }
+    }
+    cudaGraphSetConditional(h, running ? 1u : 0u);
+}
+
 // ----------------------------------------------------------------------------
 // host side
 // ----------------------------------------------------------------------------
@@ -1419,6 +1460,7 @@ template <typename C> tdda_status Krylov<C>::init(long long n3, int nrhs_) {
     for (auto b : bufs) TDDA_CUDA_TRY(cudaMalloc(b, bytes));
     TDDA_CUDA_TRY(cudaMalloc(&st, sizeof(SolverState) * nrhs));
     TDDA_CUDA_TRY(cudaMallocHost(&st_host, sizeof(SolverState) * nrhs));
+    TDDA_CUDA_TRY(cudaMalloc(&loop, sizeof(unsigned long long) * 4));
     return TDDA_OK;
 }
 
@@ -1427,9 +1469,11 @@ template <typename C> void Krylov<C>::release() {
     for (auto b : bufs) cudaFree(b);
     cudaFree(st);
     cudaFreeHost(st_host);
+    cudaFree(loop);
     r = r0 = p = t = Ap = At = nullptr;
     st = nullptr;
     st_host = nullptr;
+    loop = nullptr;
 }
 
 template <typename C>
@@ -1542,8 +1586,77 @@ tdda_status bicgstab_device(ConvOperator<C> &op, Krylov<C> &kv, const C *al, con
         return TDDA_OK;
     };
 
+    // One launch for the whole solve: the first step (p = r) directly, then a
+    // graph whose while-node repeats graph_steps iterations and the condition
+    // kernel until every right-hand side is done or the pass cap / time limit
+    // ends it.  Falls back to host-polled chunks when conditional nodes are
+    // unavailable.
+    if (o.graph_steps > 0 && o.device_loop && kv.loop != nullptr) {
+        step(true);
+        count_launches(1);
+        k_loop_start<<<1, 32, 0, s>>>(kv.loop);
+        cudaGraph_t graph = nullptr;
+        cudaGraphConditionalHandle handle;
+        bool ok = cudaGraphCreate(&graph, 0) == cudaSuccess &&
+                  cudaGraphConditionalHandleCreate(&handle, graph, 1, cudaGraphCondAssignDefault) == cudaSuccess;
+        cudaGraphNodeParams np = {};
+        cudaGraphNode_t node;
+        if (ok) {
+            np.type = cudaGraphNodeTypeConditional;
+            np.conditional.handle = handle;
+            np.conditional.type = cudaGraphCondTypeWhile;
+            np.conditional.size = 1;
+            ok = cudaGraphAddNode(&node, graph, nullptr, 0, &np) == cudaSuccess;
+        }
+        if (ok) {
+            cudaGraph_t body = np.conditional.phGraph_out[0];
+            const unsigned long long cap = (unsigned long long)max_iter / o.graph_steps + 2;
+            const unsigned long long limit_ns =
+                o.time_limit_s > 0 ? (unsigned long long)(o.time_limit_s * 1e9) : 0ull;
+            set_capturing(true);
+            cudaError_t err = cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+            if (err == cudaSuccess) {
+                for (int k = 0; k < o.graph_steps; ++k) step(false);
+                k_loop_cond<<<1, 32, 0, s>>>(handle, kv.st, nrhs, kv.loop, cap, limit_ns);
+                err = cudaStreamEndCapture(s, &body);
+            }
+            set_capturing(false);
+            if (err == cudaSuccess) err = cudaGraphInstantiate(&exec, graph, 0);
+            ok = err == cudaSuccess;
+            if (!ok) cudaGetLastError();
+        }
+        if (graph) cudaGraphDestroy(graph);
+        if (ok) {
+            TDDA_CUDA_TRY(cudaGraphLaunch(exec, s));
+            TDDA_CUDA_TRY(cudaMemcpyAsync(kv.st_host, kv.st, sizeof(SolverState) * nrhs, cudaMemcpyDeviceToHost, s));
+            unsigned long long passes = 0;
+            TDDA_CUDA_TRY(cudaMemcpyAsync(&passes, kv.loop, sizeof(passes), cudaMemcpyDeviceToHost, s));
+            TDDA_CUDA_TRY(cudaStreamSynchronize(s));
+            count_launches((long long)passes * (o.graph_steps * kLaunchesPerStep + 1));
+            if (o.fused) {
+                dim3 gu(UPD_BLOCKS, nrhs);
+                count_launches(1);
+                k_flush<C><<<gu, NT, 0, s>>>(n, X, kv.p, kv.t, kv.st);
+                TDDA_CUDA_TRY(cudaGetLastError());
+            }
+            if (info != nullptr)
+                for (int k = 0; k < nrhs; ++k) {
+                    const SolverState &S = kv.st_host[k];
+                    info[k].iterations = S.iters;
+                    info[k].error = S.err;
+                    info[k].status = S.status;
+                    info[k].refinements = 0;
+                    info[k].inner_iterations = S.iters;
+                    info[k].true_error = -1.0;
+                }
+            return TDDA_OK;
+        }
+        if (exec) { cudaGraphExecDestroy(exec); exec = nullptr; }
+        // fall back: the first step is done; continue with polled chunks
+    }
+
     long long launched = 0;
-    bool first = true;
+    bool first = !(o.graph_steps > 0 && o.device_loop && kv.loop != nullptr);
     int chunk = 2;
     for (;;) {
         if (o.graph_steps > 0 && !first) {

@@ -59,6 +59,7 @@ template <typename C> struct Krylov {
     C *r = nullptr, *r0 = nullptr, *p = nullptr, *t = nullptr, *Ap = nullptr, *At = nullptr;
     SolverState *st = nullptr;   // device
     SolverState *st_host = nullptr;  // pinned mirror
+    unsigned long long *loop = nullptr;  // device loop: passes, start time (device), and a pinned copy
     tdda_status init(long long n3, int nrhs);
     void release();
 };
@@ -70,6 +71,9 @@ struct KrylovOptions {
                                    // iterations without a 10% drop of the residual
     size_t dstride = 0;            // diagonal (al, sc) per rhs at [rhs][cell] when nbox, shared when 0
     int graph_steps = 0;           // > 0: capture this many iterations in a CUDA graph and replay it
+    bool device_loop = true;       // with graph_steps: one launch of a graph whose while-node repeats the
+                                   // iterations until every right-hand side is done (no host polls)
+    double time_limit_s = 0.0;     // device loop: end running right-hand sides with TIMEOUT after this long
     bool fused = false;            // fold the P/r update into the next iteration's first pass
                                    // (recursive residual norm from dot products; not the
                                    // reference's exact bookkeeping)

@@ -123,6 +123,7 @@ tdda_status refine_solve(const RefineWork<C> &w, const double2 *B, double2 *X, i
         o.stall_limit = kInnerStall;
         o.dstride = w.dstride;
         o.graph_steps = w.graph_steps;
+        o.time_limit_s = w.time_limit_s;
         o.fused = true;
         st = bicgstab_device<C>(*w.op, *w.kv, w.al, w.sc, w.R, w.D, nrhs, true, budget, h[2 * nrhs], s, ii.data(), o);
         if (st != TDDA_OK) return st;
@@ -132,6 +133,7 @@ tdda_status refine_solve(const RefineWork<C> &w, const double2 *B, double2 *X, i
             if (done[k]) continue;
             inner[k] += ii[k].iterations;
             refine[k] += 1;
+            if (ii[k].status == TDDA_SOLVE_TIMEOUT) { done[k] = 1; status[k] = TDDA_SOLVE_TIMEOUT; }
         }
     }
     if (info)

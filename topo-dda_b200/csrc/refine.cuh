@@ -24,6 +24,7 @@ template <typename C> struct RefineWork {
     long long nbox = 0;
     size_t dstride = 0;                     // diagonals per rhs ([rhs][cell]) when nbox
     int graph_steps = 0;                    // inner BiCGSTAB: iterations per CUDA graph (0: none)
+    double time_limit_s = 0.0;              // inner BiCGSTAB: device-side time limit (0: none)
     cudaStream_t s = nullptr;
 };
 

@@ -293,6 +293,11 @@ class DDAModel:
         k = {"none": 0, "jacobi": 1}[kind]
         _lib.check(self._lib.tdda_set_preconditioner(self._handle, k))
 
+    def setTimeLimit(self, seconds):
+        """Device-side time limit of later BiCGSTAB solves (0: none): running
+        right-hand sides end with status "timeout"."""
+        _lib.check(self._lib.tdda_set_time_limit(self._handle, float(seconds)))
+
     # --- the reference's legacy filter (models created with useFilter=True) ---
     def updateStructure(self, step, current_it, max_it):
         """DDAModel::UpdateStr (src/DDAModel.cpp:774-838) + the polarisability

@@ -18,7 +18,7 @@ STATUS_NAMES = {
     5: "CUDA error", 6: "timeout", 7: "unsupported", 8: "invalid state",
 }
 SOLVE_STATUS = {0: "running", 1: "converged", 2: "max_iter", 3: "breakdown", 4: "nonfinite",
-                5: "zero_rhs", 6: "stagnated"}
+                5: "zero_rhs", 6: "stagnated", 7: "timeout"}
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int32)
@@ -176,6 +176,7 @@ SIGNATURES = {
     "tdda_lattice_offsets_device": (ctypes.c_int, [ctypes.c_void_p, _ip, _ip, ctypes.c_void_p, ctypes.c_void_p]),
     "tdda_set_precision": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "tdda_set_preconditioner": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "tdda_set_time_limit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
     "tdda_set_solver": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "tdda_filter_update": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_int64, ctypes.c_int, ctypes.c_int]),
     "tdda_filter_gradients": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_int64, ctypes.c_int, ctypes.c_int, _dp]),
