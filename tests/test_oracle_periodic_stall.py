@@ -3,9 +3,10 @@ cell (the reason the periodic workloads use the GMRES solver).  The oracle's
 restatement of DDAModel::bicgstab (src/DDAModel.cpp:899-1009), unscaled,
 zero guess, on 40x40x10 dipoles with period 40 d and |m|,|n| <= 50, rho ~
 U[0,1] per dipole: after 1000 iterations (2000 operator applications) the
-residual is still above 1e-4 (measured: 6.0e-4), where GMRES(200) on the same
-operator is below it after 600 applications.  About three minutes of CPU on
-8 cores, so it runs only when TDDA_SLOW_TESTS=1."""
+residual is still above 1e-4 (measured: 6.0e-4).  About three minutes of CPU
+on 8 cores, so it runs only when TDDA_SLOW_TESTS=1.  (The library's GMRES
+solver reaches 1e-8 on such structures: tests/test_gpu_gmres.py,
+tests/test_gpu_configs.py.)"""
 import os
 
 import numpy as np
@@ -15,9 +16,7 @@ pytestmark = pytest.mark.skipif(os.environ.get("TDDA_SLOW_TESTS") != "1",
                                 reason="slow (minutes of CPU): set TDDA_SLOW_TESTS=1")
 
 
-def test_reference_bicgstab_stalls_where_gmres_does_not(sici):
-    import scipy.sparse.linalg as sla
-
+def test_reference_bicgstab_stalls(sici):
     from cases import model_args
     from oracle import dda_oracle as O
 
@@ -28,7 +27,3 @@ def test_reference_bicgstab_stalls_where_gmres_does_not(sici):
     ora.set_densities(rho)
     _, info = O.bicgstab(ora.aproduct_with_alb, ora.E, np.zeros(3 * ora.N, complex), 1000, 1e-8)
     assert not info.converged and info.error > 1e-4, info
-    op = sla.LinearOperator((3 * ora.N,) * 2, matvec=ora.aproduct_with_alb, dtype=complex)
-    x, _ = sla.gmres(op, ora.E, rtol=1e-12, restart=200, maxiter=3)
-    res = np.linalg.norm(ora.E - ora.aproduct_with_alb(x)) / np.linalg.norm(ora.E)
-    assert res < info.error, (res, info.error)
