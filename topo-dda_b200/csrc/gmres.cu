@@ -43,33 +43,80 @@ template <int NV> __device__ __forceinline__ void block_sum_v(double2 (&v)[NV], 
         }
 }
 
-// part[(k * nv + i) * gridDim.x + blk] = this block's share of conj(V_i[k]) . w[k]
+// part[(k * no + i) * gridDim.x + blk] = this block's share of conj(V_i[k]) . w[k]
+// for i < nv; with no = nv + 1 the CTAs of the first chunk also sum ||w[k]||^2
+// into entry i = nv
 template <typename C>
-__global__ void __launch_bounds__(kGsThreads) k_multidot(long long n, int nv, const C *__restrict__ V, size_t vstr,
-                                                         size_t rstr, const C *__restrict__ w,
+__global__ void __launch_bounds__(kGsThreads) k_multidot(long long n, int nv, int no, const C *__restrict__ V,
+                                                         size_t vstr, size_t rstr, const C *__restrict__ w,
                                                          double2 *__restrict__ part) {
     pdl_wait();
-    __shared__ double2 sm[kGsChunk * (kGsThreads / 32)];
+    __shared__ double2 sm[(kGsChunk + 1) * (kGsThreads / 32)];
     const int k = blockIdx.z, i0 = blockIdx.y * kGsChunk;
     const int nb = min(kGsChunk, nv - i0);
-    double2 acc[kGsChunk];
+    const bool norm = no > nv && blockIdx.y == 0;
+    double2 acc[kGsChunk + 1];
 #pragma unroll
-    for (int q = 0; q < kGsChunk; ++q) acc[q] = make_double2(0.0, 0.0);
+    for (int q = 0; q <= kGsChunk; ++q) acc[q] = make_double2(0.0, 0.0);
     const C *wk = w + (size_t)k * rstr;
     const C *Vk = V + (size_t)k * rstr + (size_t)i0 * vstr;
     for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
         const double2 wv = to_d(__ldg(wk + e));
+        C v[kGsChunk];
+#pragma unroll
+        for (int q = 0; q < kGsChunk; ++q)
+            if (q < nb) v[q] = __ldg(Vk + (size_t)q * vstr + e);
 #pragma unroll
         for (int q = 0; q < kGsChunk; ++q)
             if (q < nb) {
-                const double2 d = cdot1(to_d(__ldg(Vk + (size_t)q * vstr + e)), wv);
+                const double2 d = cdot1(to_d(v[q]), wv);
                 acc[q].x += d.x;
                 acc[q].y += d.y;
             }
+        if (norm) acc[kGsChunk].x += wv.x * wv.x + wv.y * wv.y;
     }
-    block_sum_v<kGsChunk>(acc, sm);
-    if (threadIdx.x == 0)
-        for (int q = 0; q < nb; ++q) part[((size_t)k * nv + i0 + q) * gridDim.x + blockIdx.x] = acc[q];
+    block_sum_v<kGsChunk + 1>(acc, sm);
+    if (threadIdx.x == 0) {
+        for (int q = 0; q < nb; ++q) part[((size_t)k * no + i0 + q) * gridDim.x + blockIdx.x] = acc[q];
+        if (norm) part[((size_t)k * no + nv) * gridDim.x + blockIdx.x] = acc[kGsChunk];
+    }
+}
+
+// out[k] = (w[k] - sum_{i < nv} c[k][i] V_i[k]) * c[k][nv].x: one Gram-Schmidt
+// update and the normalisation in one pass (c: device, rows of nv + 1)
+template <typename C>
+__global__ void __launch_bounds__(kGsThreads) k_gs_update_scale(long long n, int nv, const C *__restrict__ V,
+                                                                size_t vstr, size_t rstr,
+                                                                const double2 *__restrict__ c, C *__restrict__ w) {
+    pdl_wait();
+    extern __shared__ double2 cs[];
+    const int k = blockIdx.z;
+    for (int i = threadIdx.x; i <= nv; i += blockDim.x) cs[i] = c[(size_t)k * (nv + 1) + i];
+    __syncthreads();
+    const double f = cs[nv].x;
+    C *wk = w + (size_t)k * rstr;
+    const C *Vk = V + (size_t)k * rstr;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        double2 v = to_d(wk[e]);
+        int i = 0;
+        for (; i + 4 <= nv; i += 4) {
+            C b[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) b[q] = __ldg(Vk + (size_t)(i + q) * vstr + e);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const double2 bb = to_d(b[q]), h = cs[i + q];
+                v.x -= h.x * bb.x - h.y * bb.y;
+                v.y -= h.x * bb.y + h.y * bb.x;
+            }
+        }
+        for (; i < nv; ++i) {
+            const double2 bb = to_d(__ldg(Vk + (size_t)i * vstr + e)), h = cs[i];
+            v.x -= h.x * bb.x - h.y * bb.y;
+            v.y -= h.x * bb.y + h.y * bb.x;
+        }
+        wk[e] = from_d<C>(make_double2(f * v.x, f * v.y));
+    }
 }
 
 // out[j] = sum over blocks (in order) of part[j * nblk + b], one warp per j;
@@ -396,14 +443,14 @@ unsigned gs_blocks(long long n) {
 
 template <typename C> C *basis(GmresWork<C> &gw, int i) { return gw.V + (size_t)i * gw.n * gw.nrhs; }
 
-// h[k * nv + i] = V_i[k]^H w[k], i < nv (device)
+// h[k * (nv + 1) + i] = V_i[k]^H w[k] for i < nv and ||w[k]||^2 at i = nv (device)
 template <typename C> void multidot(GmresWork<C> &gw, int nv, const C *w, double2 *h, cudaStream_t s) {
     const size_t rstr = gw.n, vstr = (size_t)gw.n * gw.nrhs;
     const unsigned nb = gs_blocks(gw.n);
     count_launches(2);
-    launch_dep(k_multidot<C>, dim3(nb, (nv + kGsChunk - 1) / kGsChunk, gw.nrhs), dim3(kGsThreads), 0, s, gw.n, nv,
-               (const C *)gw.V, vstr, rstr, w, gw.part);
-    const int nout = gw.nrhs * nv;
+    launch_dep(k_multidot<C>, dim3(nb, std::max(1, (nv + kGsChunk - 1) / kGsChunk), gw.nrhs), dim3(kGsThreads), 0, s,
+               gw.n, nv, nv + 1, (const C *)gw.V, vstr, rstr, w, gw.part);
+    const int nout = gw.nrhs * (nv + 1);
     launch_dep(k_sum_parts, dim3((nout + 7) / 8), dim3(256), 0, s, nout, (int)nb, (const double2 *)gw.part, h,
                (double *)nullptr, (double *)nullptr);
 }
@@ -430,33 +477,51 @@ template <typename C> void scale_vec(GmresWork<C> &gw, const double *f, const C 
 }
 
 // One Arnoldi step on operator `op_fn` (v_j -> V[j+1]) with classical
-// Gram-Schmidt and one reorthogonalisation; the Hessenberg column of every
-// right-hand side lands in Hcol[k][0..j+1] (host, after the copy).
+// Gram-Schmidt: one pass for the projections and the norm of w, one pass for
+// the update and the normalisation (the new norm by Pythagoras); when the
+// update cancels more than half of w the step takes a second projection pass
+// ("twice is enough").  The Hessenberg column of every right-hand side lands
+// in Hcol[k][0..j+1].
 template <typename C, class OpFn>
 tdda_status arnoldi_step(GmresWork<C> &gw, int j, OpFn op_fn, std::vector<std::vector<cplx>> &Hcol, cudaStream_t s) {
-    const int nv = j + 1, nr = gw.nrhs, hs = gw.restart + 1;
+    const int nv = j + 1, nr = gw.nrhs;
     C *w = basis(gw, j + 1);
     tdda_status st = op_fn(basis(gw, j), w);
     if (st != TDDA_OK) return st;
-    double2 *h1 = gw.h, *h2 = gw.h + (size_t)nr * hs;
-    multidot(gw, nv, w, h1, s);
-    gs_update(gw, nv, h1, nv, w, false, s);
-    multidot(gw, nv, w, h2, s);
-    gs_update(gw, nv, h2, nv, w, true, s);
-    scale_vec(gw, gw.nrm + nr, w, w, s);
+    const size_t rstr = gw.n, vstr = (size_t)gw.n * nr;
     double2 *hh = gw.h_host;
-    TDDA_CUDA_TRY(cudaMemcpyAsync(hh, gw.h, sizeof(double2) * 2 * (size_t)nr * hs, cudaMemcpyDeviceToHost, s));
-    TDDA_CUDA_TRY(cudaMemcpyAsync(hh + 2 * (size_t)nr * hs, gw.nrm, sizeof(double) * nr, cudaMemcpyDeviceToHost, s));
-    TDDA_CUDA_TRY(cudaStreamSynchronize(s));
-    TDDA_CUDA_TRY(cudaGetLastError());
-    const double *nrm = reinterpret_cast<const double *>(hh + 2 * (size_t)nr * hs);
-    for (int k = 0; k < nr; ++k) {
-        Hcol[k].assign(nv + 1, cplx(0.0));
-        for (int i = 0; i < nv; ++i) {
-            const double2 a = hh[(size_t)k * nv + i], b = hh[(size_t)nr * hs + (size_t)k * nv + i];
-            Hcol[k][i] = cplx(a.x + b.x, a.y + b.y);
+    std::vector<double2> coef((size_t)nr * (nv + 1));
+    for (int k = 0; k < nr; ++k) Hcol[k].assign(nv + 1, cplx(0.0));
+    bool final = false;
+    for (int pass = 0; pass < 2 && !final; ++pass) {
+        multidot(gw, nv, w, gw.h, s);
+        TDDA_CUDA_TRY(cudaMemcpyAsync(hh, gw.h, sizeof(double2) * (size_t)nr * (nv + 1), cudaMemcpyDeviceToHost, s));
+        TDDA_CUDA_TRY(cudaStreamSynchronize(s));
+        TDDA_CUDA_TRY(cudaGetLastError());
+        bool cancel = false;
+        std::vector<double> wp2(nr);
+        for (int k = 0; k < nr; ++k) {
+            const double2 *hk = hh + (size_t)k * (nv + 1);
+            double proj = 0.0;
+            for (int i = 0; i < nv; ++i) {
+                proj += hk[i].x * hk[i].x + hk[i].y * hk[i].y;
+                Hcol[k][i] += cplx(hk[i].x, hk[i].y);
+                coef[(size_t)k * (nv + 1) + i] = hk[i];
+            }
+            const double wn2 = hk[nv].x;
+            wp2[k] = wn2 - proj;
+            if (wn2 > 0.0 && wp2[k] < 0.25 * wn2) cancel = true;
         }
-        Hcol[k][nv] = cplx(nrm[k], 0.0);
+        final = !cancel || pass == 1;
+        for (int k = 0; k < nr; ++k) {
+            const double nrm = final ? std::sqrt(std::max(wp2[k], 0.0)) : 1.0;
+            coef[(size_t)k * (nv + 1) + nv] = make_double2(final ? (nrm > 0.0 ? 1.0 / nrm : 0.0) : 1.0, 0.0);
+            if (final) Hcol[k][nv] = cplx(nrm, 0.0);
+        }
+        TDDA_CUDA_TRY(cudaMemcpyAsync(gw.coef, coef.data(), sizeof(double2) * coef.size(), cudaMemcpyHostToDevice, s));
+        count_launches(1);
+        launch_dep(k_gs_update_scale<C>, dim3(gs_blocks(gw.n), 1, nr), dim3(kGsThreads), sizeof(double2) * (nv + 1), s,
+                   gw.n, nv, (const C *)gw.V, vstr, rstr, (const double2 *)gw.coef, w);
     }
     return TDDA_OK;
 }
