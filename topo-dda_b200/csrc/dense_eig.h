@@ -47,30 +47,32 @@ inline void hessenberg_reduce(DenseMat &A, DenseMat *Q) {
         for (int i = k + 1; i < n; ++i) vv += std::norm(v[i]);
         if (vv == 0.0) continue;
         const double tau = 2.0 / vv;
-        // A <- H A
-        for (int j = 0; j < n; ++j) {
+        // A <- H A (columns k.. only: the earlier ones are zero below row k)
+        for (int j = k; j < n; ++j) {
+            cplx *col = &A.a[(size_t)j * n];
             cplx s = 0.0;
-            for (int i = k + 1; i < n; ++i) s += std::conj(v[i]) * A(i, j);
+            for (int i = k + 1; i < n; ++i) s += std::conj(v[i]) * col[i];
             s *= tau;
-            for (int i = k + 1; i < n; ++i) A(i, j) -= s * v[i];
+            for (int i = k + 1; i < n; ++i) col[i] -= s * v[i];
         }
-        // A <- A H
-        for (int i = 0; i < n; ++i) {
-            cplx s = 0.0;
-            for (int j = k + 1; j < n; ++j) s += A(i, j) * v[j];
-            s *= tau;
-            for (int j = k + 1; j < n; ++j) A(i, j) -= s * std::conj(v[j]);
-        }
-        for (int i = k + 2; i < n; ++i) A(i, k) = 0.0;
-        if (Q) {
-            DenseMat &q = *Q;
-            for (int i = 0; i < n; ++i) {
-                cplx s = 0.0;
-                for (int j = k + 1; j < n; ++j) s += q(i, j) * v[j];
-                s *= tau;
-                for (int j = k + 1; j < n; ++j) q(i, j) -= s * std::conj(v[j]);
+        // A <- A H, column by column (contiguous inner loops)
+        auto right = [&](DenseMat &M) {
+            std::vector<cplx> sv(n, cplx(0.0));
+            for (int j = k + 1; j < n; ++j) {
+                const cplx vj = v[j];
+                const cplx *col = &M.a[(size_t)j * n];
+                for (int i = 0; i < n; ++i) sv[i] += col[i] * vj;
             }
-        }
+            for (int i = 0; i < n; ++i) sv[i] *= tau;
+            for (int j = k + 1; j < n; ++j) {
+                const cplx cj = std::conj(v[j]);
+                cplx *col = &M.a[(size_t)j * n];
+                for (int i = 0; i < n; ++i) col[i] -= sv[i] * cj;
+            }
+        };
+        right(A);
+        for (int i = k + 2; i < n; ++i) A(i, k) = 0.0;
+        if (Q) right(*Q);
     }
 }
 
