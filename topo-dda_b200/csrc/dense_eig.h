@@ -33,6 +33,10 @@ inline void hessenberg_reduce(DenseMat &A, DenseMat *Q) {
     }
     std::vector<cplx> v(n);
     for (int k = 0; k + 2 < n; ++k) {
+        // a column already zero below its subdiagonal needs no reflector
+        bool zero_below = true;
+        for (int i = k + 2; i < n && zero_below; ++i) zero_below = A(i, k) == cplx(0.0);
+        if (zero_below) continue;
         double alpha2 = 0.0;
         for (int i = k + 1; i < n; ++i) alpha2 += std::norm(A(i, k));
         const double xnorm = std::sqrt(alpha2);
@@ -191,6 +195,74 @@ bool eigenpairs(DenseMat A, std::vector<cplx> &ev, std::vector<std::vector<cplx>
         nr = std::sqrt(nr);
         if (nr > 0)
             for (auto &e : v) e /= nr;
+        vecs.push_back(v);
+    }
+    return true;
+}
+
+// Solves (H - theta I) x = b for the upper-Hessenberg H (column-major;
+// Gaussian elimination with pivoting between neighbouring rows, O(n^2)); a
+// zero pivot is replaced by a tiny one (theta may be an eigenvalue).
+inline std::vector<cplx> hessenberg_shifted_solve(const DenseMat &H, cplx theta, std::vector<cplx> b) {
+    const int n = H.n;
+    DenseMat A = H;
+    for (int i = 0; i < n; ++i) A(i, i) -= theta;
+    double scale = 0.0;
+    for (int i = 0; i < n; ++i) scale = std::max(scale, std::abs(H(i, i)));
+    const double tiny = 1e-14 * (scale > 0 ? scale : 1.0);
+    for (int k = 0; k + 1 < n; ++k) {
+        if (std::abs(A(k + 1, k)) > std::abs(A(k, k))) {
+            for (int j = k; j < n; ++j) std::swap(A(k, j), A(k + 1, j));
+            std::swap(b[k], b[k + 1]);
+        }
+        if (std::abs(A(k, k)) < tiny) A(k, k) = tiny;
+        const cplx f = A(k + 1, k) / A(k, k);
+        if (f != cplx(0.0)) {
+            for (int j = k; j < n; ++j) A(k + 1, j) -= f * A(k, j);
+            b[k + 1] -= f * b[k];
+        }
+    }
+    if (std::abs(A(n - 1, n - 1)) < tiny) A(n - 1, n - 1) = tiny;
+    std::vector<cplx> x(n);
+    for (int i = n - 1; i >= 0; --i) {
+        cplx t = b[i];
+        for (int j = i + 1; j < n; ++j) t -= A(i, j) * x[j];
+        x[i] = t / A(i, i);
+    }
+    return x;
+}
+
+// As eigenpairs, for a few eigenvectors: the eigenvalues from the QR
+// iteration without Schur vectors, the selected eigenvectors by two steps of
+// inverse iteration on the Hessenberg form, mapped back through the
+// reduction's reflections.  Much cheaper when few vectors are wanted.
+template <class Pick>
+bool eigenpairs_few(DenseMat A, std::vector<cplx> &ev, std::vector<std::vector<cplx>> &vecs, Pick pick) {
+    const int n = A.n;
+    DenseMat Q;
+    hessenberg_reduce(A, &Q);
+    DenseMat H = A;
+    if (!hessenberg_qr(H, nullptr)) return false;
+    ev.resize(n);
+    for (int i = 0; i < n; ++i) ev[i] = H(i, i);
+    const std::vector<int> idx = pick(ev);
+    vecs.clear();
+    for (int p : idx) {
+        std::vector<cplx> x(n, cplx(1.0 / std::sqrt((double)n)));
+        for (int it = 0; it < 2; ++it) {
+            x = hessenberg_shifted_solve(A, ev[p], x);
+            double nr = 0.0;
+            for (auto &e : x) nr += std::norm(e);
+            nr = std::sqrt(nr);
+            if (!(nr > 0.0) || !std::isfinite(nr)) return false;
+            for (auto &e : x) e /= nr;
+        }
+        std::vector<cplx> v(n, cplx(0.0));
+        for (int j = 0; j < n; ++j) {
+            const cplx xj = x[j];
+            const cplx *col = &Q.a[(size_t)j * n];
+            for (int i = 0; i < n; ++i) v[i] += col[i] * xj;
+        }
         vecs.push_back(v);
     }
     return true;

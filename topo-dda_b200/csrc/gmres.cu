@@ -621,7 +621,7 @@ int deflated_restart(LsqState &L, int kd, const std::vector<cplx> &y, std::vecto
             const double h2 = std::norm(L.h(m, m - 1));
             for (int i = 0; i < m; ++i) M(i, m - 1) += h2 * f[i];
             std::vector<cplx> ev;
-            ok = eigenpairs(M, ev, cols, [&](const std::vector<cplx> &e) {
+            ok = eigenpairs_few(M, ev, cols, [&](const std::vector<cplx> &e) {
                 std::vector<int> id(e.size());
                 for (size_t i = 0; i < e.size(); ++i) id[i] = (int)i;
                 std::sort(id.begin(), id.end(), [&](int a, int b) { return std::abs(e[a]) < std::abs(e[b]); });
