@@ -537,9 +537,6 @@ static tdda_status ensure_op_cap(tdda_model *m, int nrhs) {
     cudaFree(m->op.T);
     m->op.T = nullptr;
     TDDA_CUDA_TRY(cudaMalloc(&m->op.T, sizeof(double2) * (size_t)nrhs * 3 * m->op.g.tcomp));
-    cudaFree(m->op.U);
-    m->op.U = nullptr;
-    if (m->op.g.split_yz) TDDA_CUDA_TRY(cudaMalloc(&m->op.U, split_bytes(m->op.g, nrhs, sizeof(double2))));
     cudaFree(m->op.partials);
     cudaFree(m->op.counters);
     m->op.partials = nullptr;

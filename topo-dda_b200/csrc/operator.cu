@@ -33,7 +33,6 @@ constexpr int NT = 512;          // threads per CTA of the convolution passes
 constexpr int MAXI = 2;          // FFT work items a thread holds per stage
 constexpr int SMEM_MAX = 200 * 1024;
 constexpr int UPD_BLOCKS = 296;  // 2 x 148 SMs for the element-wise update
-constexpr int kSmemSplit = 100 * 1024;  // shared-memory cap of a split-pass tile (two CTAs per SM)
 
 // ----------------------------------------------------------------------------
 // deterministic reductions
@@ -694,139 +693,6 @@ __global__ void __launch_bounds__(NT) k_inv_yz(ConvGeom g, const C *__restrict__
 }
 
 // ----------------------------------------------------------------------------
-// passes 1 and 3 split in two kernels each (complex128 slabs, which do not fit
-// the register slab kernels): the z transforms and the y transforms run as
-// separate kernels with U[(rhs, c, x)][kz][y] (ny * Lz per slab) between
-// them, so that each kernel holds a small tile (a few dozen KB of shared
-// memory, several CTAs per SM) instead of a whole slab per CTA.
-// ----------------------------------------------------------------------------
-constexpr int NTU = 256;
-
-// pass 1a: (x, rows y0 .. y0+YU, c, rhs): prologue, zero-padded z transforms,
-// spectra to U[kz][y]
-template <typename C, class Pro>
-__global__ void __launch_bounds__(NTU) k_fwd_z(ConvGeom g, C *__restrict__ U, const C *__restrict__ tw, Pro pro) {
-    pdl_wait();
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    C *A = reinterpret_cast<C *>(smem_raw);  // [y local][kz], pitch Lz + 1
-    const int nyb = (g.ny + g.YU - 1) / g.YU;
-    const int x = blockIdx.x / nyb, y0 = (blockIdx.x - x * nyb) * g.YU, c = blockIdx.y, rhs = blockIdx.z;
-    if (pro.skip(rhs)) return;
-    const int nyl = min(g.YU, g.ny - y0), pz = g.Lz + 1;
-    const long long cell0 = ((long long)x * g.ny + y0) * g.nz;
-    for (int e = threadIdx.x; e < nyl * g.nz; e += NTU) {
-        const int yl = e / g.nz, z = e - yl * g.nz;
-        A[yl * pz + z] = pro.load(rhs, c, cell0 + e);
-    }
-    const int zpad = g.Lz - g.nz;
-    for (int e = threadIdx.x; e < nyl * zpad; e += NTU) {
-        const int yl = e / zpad, z = g.nz + (e - yl * zpad);
-        A[yl * pz + z] = czero<C>();
-    }
-    __syncthreads();
-    fft_smem<-1, MAXI>(A, g.Lz, nyl, 1, pz, tw, g.Lmax);
-    C *Us = U + ((size_t)(rhs * 3 + c) * g.nx + x) * (size_t)g.Lz * g.ny;
-    for (int e = threadIdx.x; e < g.Lz * nyl; e += NTU) {
-        const int kz = e / nyl, yl = e - kz * nyl;
-        Us[(size_t)kz * g.ny + y0 + yl] = A[yl * pz + kz];
-    }
-}
-
-// pass 1b: (x, kz0 .. kz0+KU, c, rhs): zero-padded y transforms from U to T[ky][kz]
-template <typename C>
-__global__ void __launch_bounds__(NTU) k_fwd_y(ConvGeom g, const C *__restrict__ U, C *__restrict__ T,
-                                               const C *__restrict__ tw, const SolverState *__restrict__ st) {
-    pdl_wait();
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    C *Bs = reinterpret_cast<C *>(smem_raw);  // [kz local][ky], pitch Ly + 1
-    const int nkb = (g.Lz + g.KU - 1) / g.KU;
-    const int x = blockIdx.x, c = blockIdx.y / nkb, kz0 = (blockIdx.y - c * nkb) * g.KU, rhs = blockIdx.z;
-    if (st != nullptr && st[rhs].done) return;
-    const int nk = min(g.KU, g.Lz - kz0), py = g.Ly + 1;
-    const size_t slab = (size_t)(rhs * 3 + c) * g.nx + x;
-    const C *Us = U + slab * (size_t)g.Lz * g.ny;
-    for (int e = threadIdx.x; e < nk * g.ny; e += NTU) {
-        const int kl = e / g.ny, y = e - kl * g.ny;
-        Bs[kl * py + y] = Us[(size_t)(kz0 + kl) * g.ny + y];
-    }
-    const int ypad = g.Ly - g.ny;
-    for (int e = threadIdx.x; e < nk * ypad; e += NTU) {
-        const int kl = e / ypad, y = g.ny + (e - kl * ypad);
-        Bs[kl * py + y] = czero<C>();
-    }
-    __syncthreads();
-    fft_smem<-1, MAXI>(Bs, g.Ly, nk, 1, py, tw, g.Lmax);
-    C *Tc = T + slab * (size_t)g.Ly * g.Lz;
-    for (int e = threadIdx.x; e < g.Ly * nk; e += NTU) {
-        const int ky = e / nk, kl = e - ky * nk;
-        Tc[(size_t)ky * g.Lz + kz0 + kl] = Bs[kl * py + ky];
-    }
-}
-
-// pass 3a: (x, kz0 .. kz0+KU, c, rhs): inverse y transforms from T, rows y < ny to U[kz][y]
-template <typename C>
-__global__ void __launch_bounds__(NTU) k_inv_y(ConvGeom g, const C *__restrict__ T, C *__restrict__ U,
-                                               const C *__restrict__ tw, const SolverState *__restrict__ st) {
-    pdl_wait();
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    C *Bs = reinterpret_cast<C *>(smem_raw);  // [kz local][ky], pitch Ly + 1
-    const int nkb = (g.Lz + g.KU - 1) / g.KU;
-    const int x = blockIdx.x, c = blockIdx.y / nkb, kz0 = (blockIdx.y - c * nkb) * g.KU, rhs = blockIdx.z;
-    if (st != nullptr && st[rhs].done) return;
-    const int nk = min(g.KU, g.Lz - kz0), py = g.Ly + 1;
-    const size_t slab = (size_t)(rhs * 3 + c) * g.nx + x;
-    const C *Tc = T + slab * (size_t)g.Ly * g.Lz;
-    for (int e = threadIdx.x; e < g.Ly * nk; e += NTU) {
-        const int ky = e / nk, kl = e - ky * nk;
-        Bs[kl * py + ky] = Tc[(size_t)ky * g.Lz + kz0 + kl];
-    }
-    __syncthreads();
-    fft_smem<+1, MAXI>(Bs, g.Ly, nk, 1, py, tw, g.Lmax);
-    C *Us = U + slab * (size_t)g.Lz * g.ny;
-    for (int e = threadIdx.x; e < nk * g.ny; e += NTU) {
-        const int kl = e / g.ny, y = e - kl * g.ny;
-        Us[(size_t)(kz0 + kl) * g.ny + y] = Bs[kl * py + y];
-    }
-}
-
-// pass 3b: one CTA per (x, c, rhs) slab, rows in chunks of YU: inverse z
-// transforms from U, the crop z < nz and the fused epilogue (one CTA per slab
-// keeps the epilogue's block partials and their order as in k_inv_yz)
-template <typename C, class Epi>
-__global__ void __launch_bounds__(NTU) k_inv_z(ConvGeom g, const C *__restrict__ U, const C *__restrict__ tw,
-                                               Epi epi) {
-    pdl_wait();
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    C *A = reinterpret_cast<C *>(smem_raw);  // [y local][kz], pitch Lz + 1
-    const int x = blockIdx.x, c = blockIdx.y, rhs = blockIdx.z;
-    if (epi.skip(rhs)) return;
-    const int pz = g.Lz + 1;
-    const C *Us = U + ((size_t)(rhs * 3 + c) * g.nx + x) * (size_t)g.Lz * g.ny;
-    double2 acc[Epi::NQ > 0 ? Epi::NQ : 1];
-#pragma unroll
-    for (int q = 0; q < (Epi::NQ > 0 ? Epi::NQ : 1); ++q) acc[q] = make_double2(0.0, 0.0);
-    for (int y0 = 0; y0 < g.ny; y0 += g.YU) {
-        const int nyl = min(g.YU, g.ny - y0);
-        for (int e = threadIdx.x; e < g.Lz * nyl; e += NTU) {
-            const int kz = e / nyl, yl = e - kz * nyl;
-            A[yl * pz + kz] = Us[(size_t)kz * g.ny + y0 + yl];
-        }
-        __syncthreads();
-        fft_smem<+1, MAXI>(A, g.Lz, nyl, 1, pz, tw, g.Lmax);
-        const long long cell0 = ((long long)x * g.ny + y0) * g.nz;
-        for (int e = threadIdx.x; e < nyl * g.nz; e += NTU) {
-            const int yl = e / g.nz, z = e - yl * g.nz;
-            epi.apply(rhs, c, cell0 + e, A[yl * pz + z], acc);
-        }
-        __syncthreads();
-    }
-    if constexpr (Epi::NQ > 0) {
-        reduce_finalize<Epi::NQ>(acc, epi.part + (size_t)rhs * epi.pstride, epi.counter + rhs,
-                                 blockIdx.y * gridDim.x + blockIdx.x, gridDim.x * gridDim.y, epi, rhs);
-    }
-}
-
-// ----------------------------------------------------------------------------
 // prologues (what pass 1 transforms) and epilogues (what pass 3 produces)
 // ----------------------------------------------------------------------------
 // Optional diagonal (Jacobi) scaling: with sc = D^(-1/2) per cell the passes
@@ -1296,19 +1162,6 @@ template <typename C> static void set_smem_attrs(int yz, int x) {
     cudaFuncSetAttribute(k_inv_yz<C, EpiInit<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, yz);
     cudaFuncSetAttribute(k_inv_yz<C, EpiAp<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, yz);
     cudaFuncSetAttribute(k_inv_yz<C, EpiAt<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, yz);
-    // split passes (tiles of at most 100 KB)
-    cudaFuncSetAttribute(k_fwd_z<C, ProLoad<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemSplit);
-    cudaFuncSetAttribute(k_fwd_z<C, ProP<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemSplit);
-    cudaFuncSetAttribute(k_fwd_z<C, ProT<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemSplit);
-    cudaFuncSetAttribute(k_fwd_z<C, ProPF<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemSplit);
-    cudaFuncSetAttribute(k_fwd_y<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemSplit);
-    cudaFuncSetAttribute(k_inv_y<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemSplit);
-    cudaFuncSetAttribute(k_inv_z<C, EpiAtF<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemSplit);
-    cudaFuncSetAttribute(k_inv_z<C, EpiMatvec<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemSplit);
-    cudaFuncSetAttribute(k_inv_z<C, EpiPoly<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemSplit);
-    cudaFuncSetAttribute(k_inv_z<C, EpiInit<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemSplit);
-    cudaFuncSetAttribute(k_inv_z<C, EpiAp<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemSplit);
-    cudaFuncSetAttribute(k_inv_z<C, EpiAt<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemSplit);
     cudaFuncSetAttribute(k_xconv<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, x);
     cudaFuncSetAttribute(k_xconv_fast<C, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, x);
     cudaFuncSetAttribute(k_xconv_fast<C, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, x);
@@ -1452,28 +1305,6 @@ static bool plan_geom(int nx, int ny, int nz, int nrhs, int esize, ConvGeom &g, 
         }
     }
     if (g.CKx == 0 && !g.fast_x && !g.reg_x) { why = "x pencils do not fit in shared memory"; return false; }
-    // complex128 slabs (no register slab kernel): split passes 1 and 3
-    g.split_yz = 0;
-    g.YU = g.KU = 0;
-    if (esize == 16 && !g.reg_yz && !g.fast_yz) {
-        for (int yu = std::min(ny, 128); yu >= 1; --yu) {
-            if ((long long)yu * (g.Lz + 1) * esize > kSmemSplit) continue;
-            if (fft_max_items(g.Lz, yu, NTU) > MAXI) continue;
-            g.YU = yu;
-            break;
-        }
-        for (int ku = std::min(g.Lz, 32); ku >= 1; --ku) {
-            if ((long long)ku * (g.Ly + 1) * esize > kSmemSplit) continue;
-            if (fft_max_items(g.Ly, ku, NTU) > MAXI) continue;
-            g.KU = ku;
-            break;
-        }
-        if (g.YU > 0 && g.KU > 0) {
-            g.split_yz = 1;
-            g.smem_uz = (int)((long long)g.YU * (g.Lz + 1) * esize);
-            g.smem_uy = (int)((long long)g.KU * (g.Ly + 1) * esize);
-        }
-    }
     return true;
 }
 
@@ -1495,7 +1326,6 @@ template <typename C> tdda_status ConvOperator<C>::init(int nx, int ny, int nz, 
     TDDA_CUDA_TRY(cudaMalloc(&tw, sizeof(C) * g.Lmax));
     TDDA_CUDA_TRY(cudaMemcpy(tw, h.data(), sizeof(C) * g.Lmax, cudaMemcpyHostToDevice));
     TDDA_CUDA_TRY(cudaMalloc(&T, sizeof(C) * (size_t)nrhs_cap * 3 * g.tcomp));
-    if (g.split_yz) TDDA_CUDA_TRY(cudaMalloc(&U, split_bytes(g, nrhs_cap, sizeof(C))));
     partial_cap = std::max(3 * nx, UPD_BLOCKS) * kMaxNQ;
     TDDA_CUDA_TRY(cudaMalloc(&partials, sizeof(double2) * (size_t)partial_cap * nrhs_cap));
     TDDA_CUDA_TRY(cudaMalloc(&counters, sizeof(unsigned) * (size_t)nrhs_cap));
@@ -1503,17 +1333,13 @@ template <typename C> tdda_status ConvOperator<C>::init(int nx, int ny, int nz, 
     return TDDA_OK;
 }
 
-size_t split_bytes(const ConvGeom &g, int nrhs_cap, size_t esize) {
-    return g.split_yz ? esize * (size_t)nrhs_cap * 3 * g.nx * g.Lz * g.ny : 0;
-}
-
 size_t conv_workspace_bytes(int nx, int ny, int nz, int nrhs_cap, int esize) {
     ConvGeom g;
     std::string why;
     if (!plan_geom(nx, ny, nz, 1, esize, g, why)) return 0;
     const size_t partial_cap = (size_t)std::max(3 * nx, UPD_BLOCKS) * kMaxNQ;
-    return (size_t)esize * g.Lmax + (size_t)esize * nrhs_cap * 3 * g.tcomp + split_bytes(g, nrhs_cap, esize) +
-           sizeof(double2) * partial_cap * nrhs_cap + sizeof(unsigned) * nrhs_cap;
+    return (size_t)esize * g.Lmax + (size_t)esize * nrhs_cap * 3 * g.tcomp + sizeof(double2) * partial_cap * nrhs_cap +
+           sizeof(unsigned) * nrhs_cap;
 }
 
 bool conv_supported(int nx, int ny, int nz, int nrhs, int esize, std::string &why) {
@@ -1522,8 +1348,8 @@ bool conv_supported(int nx, int ny, int nz, int nrhs, int esize, std::string &wh
 }
 
 template <typename C> void ConvOperator<C>::release() {
-    cudaFree(ahat); cudaFree(tw); cudaFree(T); cudaFree(U); cudaFree(partials); cudaFree(counters);
-    ahat = nullptr; tw = nullptr; T = nullptr; U = nullptr; partials = nullptr; counters = nullptr;
+    cudaFree(ahat); cudaFree(tw); cudaFree(T); cudaFree(partials); cudaFree(counters);
+    ahat = nullptr; tw = nullptr; T = nullptr; partials = nullptr; counters = nullptr;
 }
 
 template <typename C> static bool geom_for(const ConvOperator<C> &op, int nrhs, ConvGeom &g) {
@@ -1536,15 +1362,9 @@ template <typename C, class Pro, class Epi>
 static tdda_status run_conv(ConvOperator<C> &op, const ConvGeom &g, int nrhs, const Pro &pro,
                             const Epi &epi, const SolverState *st, cudaStream_t s) {
     dim3 g13(g.nx, 3, nrhs);
-    const bool split = g.split_yz && op.U != nullptr;
-    const int nyb = split ? (g.ny + g.YU - 1) / g.YU : 0, nkb = split ? (g.Lz + g.KU - 1) / g.KU : 0;
     count_launches(1);
-    if (split) {
-        launch_dep((k_fwd_z<C, Pro>), dim3(g.nx * nyb, 3, nrhs), dim3(NTU), g.smem_uz, s, g, op.U, op.tw, pro);
-        count_launches(1);
-        launch_dep(k_fwd_y<C>, dim3(g.nx, 3 * nkb, nrhs), dim3(NTU), g.smem_uy, s, g, (const C *)op.U, op.T, op.tw, st);
-    } else if (!launch_fwd_reg<C, Pro>(g, g13, op.T, op.tw, pro, s) &&
-               !(g.fast_yz && launch_fwd_fast<C, Pro>(g, g13, op.T, op.tw, pro, s)))
+    if (!launch_fwd_reg<C, Pro>(g, g13, op.T, op.tw, pro, s) &&
+        !(g.fast_yz && launch_fwd_fast<C, Pro>(g, g13, op.T, op.tw, pro, s)))
         launch_dep((k_fwd_zy<C, Pro>), g13, dim3(NT), g.smem_yz, s, g, op.T, op.tw, pro);
     dim3 g2(g.Ly, g.CKx > 0 ? g.Lz / g.CKx : 1, 1);
     count_launches(1);
@@ -1552,12 +1372,8 @@ static tdda_status run_conv(ConvOperator<C> &op, const ConvGeom &g, int nrhs, co
         !(g.fast_x && launch_xconv_fast<C>(g, op.T, op.ahat, op.ahat_rhs, op.tw, nrhs, st, s)))
         launch_dep(k_xconv<C>, g2, dim3(NT), g.smem_x, s, g, op.T, op.ahat, op.ahat_rhs, op.tw, nrhs, st);
     count_launches(1);
-    if (split) {
-        launch_dep(k_inv_y<C>, dim3(g.nx, 3 * nkb, nrhs), dim3(NTU), g.smem_uy, s, g, (const C *)op.T, op.U, op.tw, st);
-        count_launches(1);
-        launch_dep((k_inv_z<C, Epi>), g13, dim3(NTU), g.smem_uz, s, g, (const C *)op.U, op.tw, epi);
-    } else if (!launch_inv_reg<C, Epi>(g, g13, op.T, op.tw, epi, s) &&
-               !(g.fast_yz && launch_inv_fast<C, Epi>(g, g13, op.T, op.tw, epi, s)))
+    if (!launch_inv_reg<C, Epi>(g, g13, op.T, op.tw, epi, s) &&
+        !(g.fast_yz && launch_inv_fast<C, Epi>(g, g13, op.T, op.tw, epi, s)))
         launch_dep((k_inv_yz<C, Epi>), g13, dim3(NT), g.smem_yz, s, g, op.T, op.tw, epi);
     return TDDA_OK;
 }
@@ -1624,7 +1440,6 @@ tdda_status apply_external_scratch(const ConvOperator<C> &op, C *T_ext, const C 
                                    cudaStream_t s) {
     ConvOperator<C> view = op;  // same tensor, twiddles and plan; only the intermediate moves
     view.T = T_ext;
-    view.U = nullptr;           // one slab kernel per pass: no second intermediate
     ProLoad<C> pro{};
     pro.nbox = op.g.nbox; pro.x = x; pro.st = nullptr;
     EpiMatvec<C> epi{};
@@ -1925,15 +1740,9 @@ tdda_status profile_apply(ConvOperator<C> &op, const C *x, C *y, const C *al, in
         return (double)ms / iters;
     };
     *ms_total = timed([&] { run_conv(op, g, nrhs, pro, epi, nullptr, s); });
-    const bool split = g.split_yz && op.U != nullptr;
-    const int nyb = split ? (g.ny + g.YU - 1) / g.YU : 0, nkb = split ? (g.Lz + g.KU - 1) / g.KU : 0;
     ms_pass[0] = timed([&] {
         count_launches(1);
-        if (split) {
-            count_launches(1);
-            k_fwd_z<C, ProLoad<C>><<<dim3(g.nx * nyb, 3, nrhs), NTU, g.smem_uz, s>>>(g, op.U, op.tw, pro);
-            k_fwd_y<C><<<dim3(g.nx, 3 * nkb, nrhs), NTU, g.smem_uy, s>>>(g, op.U, op.T, op.tw, nullptr);
-        } else if (!launch_fwd_reg<C, ProLoad<C>>(g, g13, op.T, op.tw, pro, s) &&
+        if (!launch_fwd_reg<C, ProLoad<C>>(g, g13, op.T, op.tw, pro, s) &&
             !(g.fast_yz && launch_fwd_fast<C, ProLoad<C>>(g, g13, op.T, op.tw, pro, s)))
             k_fwd_zy<C, ProLoad<C>><<<g13, NT, g.smem_yz, s>>>(g, op.T, op.tw, pro);
     });
@@ -1945,11 +1754,7 @@ tdda_status profile_apply(ConvOperator<C> &op, const C *x, C *y, const C *al, in
     });
     ms_pass[2] = timed([&] {
         count_launches(1);
-        if (split) {
-            count_launches(1);
-            k_inv_y<C><<<dim3(g.nx, 3 * nkb, nrhs), NTU, g.smem_uy, s>>>(g, op.T, op.U, op.tw, nullptr);
-            k_inv_z<C, EpiMatvec<C>><<<g13, NTU, g.smem_uz, s>>>(g, op.U, op.tw, epi);
-        } else if (!launch_inv_reg<C, EpiMatvec<C>>(g, g13, op.T, op.tw, epi, s) &&
+        if (!launch_inv_reg<C, EpiMatvec<C>>(g, g13, op.T, op.tw, epi, s) &&
             !(g.fast_yz && launch_inv_fast<C, EpiMatvec<C>>(g, g13, op.T, op.tw, epi, s)))
             k_inv_yz<C, EpiMatvec<C>><<<g13, NT, g.smem_yz, s>>>(g, op.T, op.tw, epi);
     });

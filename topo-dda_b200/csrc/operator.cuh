@@ -34,7 +34,6 @@ template <typename C> struct ConvOperator {
     const C *const *ahat_rhs = nullptr;  // device table of one tensor per right-hand side, or nullptr
     C *tw = nullptr;       // twiddles exp(-2 pi i j / Lmax), j < Lmax
     C *T = nullptr;        // spectral intermediate, nrhs_cap * 3 * tcomp
-    C *U = nullptr;        // z-transformed slabs between split passes, nrhs_cap * 3 * nx * Lz * ny (g.split_yz)
     int nrhs_cap = 0;
     double2 *partials = nullptr;  // reduction scratch
     unsigned *counters = nullptr; // last-block counters
@@ -50,8 +49,6 @@ template <typename C> struct ConvOperator {
 // Device bytes ConvOperator<C>::init allocates (twiddles, spectral
 // intermediate, reduction scratch; not the tensor) for esize = sizeof(C).
 size_t conv_workspace_bytes(int nx, int ny, int nz, int nrhs_cap, int esize);
-// Bytes of the split passes' intermediate U (0 when the plan does not split).
-size_t split_bytes(const ConvGeom &g, int nrhs_cap, size_t esize);
 // Whether the fused operator supports this grid with nrhs right-hand sides.
 bool conv_supported(int nx, int ny, int nz, int nrhs, int esize, std::string &why);
 

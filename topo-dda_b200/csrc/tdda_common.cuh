@@ -102,9 +102,6 @@ struct ConvGeom {
     int fast_x;         // 1: pass 2 uses the compile-time-length kernel for Lx
     int CKx2;           // kz chunk of that kernel
     int smem_x2;        // its dynamic SMEM bytes (two ping-pong buffers)
-    int split_yz;       // 1: passes 1 and 3 as separate z and y transform kernels through U
-    int YU, KU;         // y rows per z-transform CTA, kz columns per y-transform CTA
-    int smem_uz, smem_uy;  // their dynamic SMEM bytes
 };
 
 // ----------------------------------------------------------------------------
