@@ -89,7 +89,34 @@ def parse():
     ap.add_argument("--profile-matvec", type=int, default=0, metavar="K",
                     help="only build the benchmark model and apply the operator K times per precision "
                          "(the case the kernel profiles capture); prints per-pass times")
+    ap.add_argument("--profile-gmres", type=int, default=0, metavar="K",
+                    help="profile case of the GMRES-DR kernels: one mixed-precision solve of the x-polarised "
+                         "RHS on the 64x64x16 periodic structure (period 64 d, |m|,|n| <= 50), capped at K "
+                         "inner operator applications; prints the solve record")
     return ap.parse_args()
+
+
+def run_profile_gmres(k, sici):
+    """A short GMRES-DR solve on a quarter-size periodic cell (the case the
+    Gram-Schmidt kernel profiles capture: same kernels, same basis length per
+    dipole, 3 * 64 * 64 * 16 unknowns per vector)."""
+    import torch
+
+    from dda_model import DDAModel
+
+    w = dict(WORKLOAD, nx=64, ny=64, nz=16, period=64)
+    m = DDAModel(**model_kwargs(w, sici), precision="mixed")
+    m.setDensities(design(w))
+    m.setSolver("pgmres", **SOLVER)
+    B = torch.from_numpy(np.stack([incident(w, 0)])).cuda()
+    X = torch.zeros_like(B)
+    s = torch.cuda.current_stream()
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    info = m.solve_batch_device(B.data_ptr(), X.data_ptr(), 1, True, k, w["tol"], s.cuda_stream)[0]
+    torch.cuda.synchronize()
+    print(json.dumps(dict(grid=[64, 64, 16], M=w["M"], seconds=time.perf_counter() - t, **info)))
+    return 0
 
 
 def workload(small=False):
@@ -719,6 +746,8 @@ def main():
 
     w = workload(args.small)
     sici = dda_model.sici_tables()
+    if args.profile_gmres > 0:
+        return run_profile_gmres(args.profile_gmres, sici)
     rho = design(w)
     t0 = time.perf_counter()
     pair = PolPair(w, sici, rho, solver=SOLVER, device=f"cuda:{local}")

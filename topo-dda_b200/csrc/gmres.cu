@@ -45,7 +45,10 @@ template <int NV> __device__ __forceinline__ void block_sum_v(double2 (&v)[NV], 
 
 // part[(k * no + i) * gridDim.x + blk] = this block's share of conj(V_i[k]) . w[k]
 // for i < nv; with no = nv + 1 the CTAs of the first chunk also sum ||w[k]||^2
-// into entry i = nv
+// into entry i = nv.  A thread takes kMdElems elements per round and issues
+// the loads of all of them (kGsChunk basis vectors each) before using any.
+constexpr int kMdElems = 2;
+
 template <typename C>
 __global__ void __launch_bounds__(kGsThreads) k_multidot(long long n, int nv, int no, const C *__restrict__ V,
                                                          size_t vstr, size_t rstr, const C *__restrict__ w,
@@ -60,20 +63,28 @@ __global__ void __launch_bounds__(kGsThreads) k_multidot(long long n, int nv, in
     for (int q = 0; q <= kGsChunk; ++q) acc[q] = make_double2(0.0, 0.0);
     const C *wk = w + (size_t)k * rstr;
     const C *Vk = V + (size_t)k * rstr + (size_t)i0 * vstr;
-    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
-        const double2 wv = to_d(__ldg(wk + e));
-        C v[kGsChunk];
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long e0 = (long long)blockIdx.x * blockDim.x + threadIdx.x; e0 < n; e0 += kMdElems * stride) {
+        C wv[kMdElems], v[kMdElems][kGsChunk];
 #pragma unroll
-        for (int q = 0; q < kGsChunk; ++q)
-            if (q < nb) v[q] = __ldg(Vk + (size_t)q * vstr + e);
+        for (int u = 0; u < kMdElems; ++u) {
+            const long long e = e0 + u * stride;
+            const bool in = e < n;
+            wv[u] = in ? __ldg(wk + e) : czero<C>();
 #pragma unroll
-        for (int q = 0; q < kGsChunk; ++q)
-            if (q < nb) {
-                const double2 d = cdot1(to_d(v[q]), wv);
+            for (int q = 0; q < kGsChunk; ++q) v[u][q] = (in && q < nb) ? __ldg(Vk + (size_t)q * vstr + e) : czero<C>();
+        }
+#pragma unroll
+        for (int u = 0; u < kMdElems; ++u) {
+            const double2 wd = to_d(wv[u]);
+#pragma unroll
+            for (int q = 0; q < kGsChunk; ++q) {
+                const double2 d = cdot1(to_d(v[u][q]), wd);
                 acc[q].x += d.x;
                 acc[q].y += d.y;
             }
-        if (norm) acc[kGsChunk].x += wv.x * wv.x + wv.y * wv.y;
+            if (norm) acc[kGsChunk].x += wd.x * wd.x + wd.y * wd.y;
+        }
     }
     block_sum_v<kGsChunk + 1>(acc, sm);
     if (threadIdx.x == 0) {
@@ -83,7 +94,11 @@ __global__ void __launch_bounds__(kGsThreads) k_multidot(long long n, int nv, in
 }
 
 // out[k] = (w[k] - sum_{i < nv} c[k][i] V_i[k]) * c[k][nv].x: one Gram-Schmidt
-// update and the normalisation in one pass (c: device, rows of nv + 1)
+// update and the normalisation in one pass (c: device, rows of nv + 1).  A
+// thread updates kUpElems elements at once and issues their loads of four
+// basis vectors together (16 loads in flight per thread).
+constexpr int kUpElems = 4;
+
 template <typename C>
 __global__ void __launch_bounds__(kGsThreads) k_gs_update_scale(long long n, int nv, const C *__restrict__ V,
                                                                 size_t vstr, size_t rstr,
@@ -96,26 +111,45 @@ __global__ void __launch_bounds__(kGsThreads) k_gs_update_scale(long long n, int
     const double f = cs[nv].x;
     C *wk = w + (size_t)k * rstr;
     const C *Vk = V + (size_t)k * rstr;
-    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
-        double2 v = to_d(wk[e]);
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long e0 = (long long)blockIdx.x * blockDim.x + threadIdx.x; e0 < n; e0 += kUpElems * stride) {
+        double2 acc[kUpElems];
+        // elements u < nin of this round lie inside the vector
+        const long long left = (n - e0 + stride - 1) / stride;
+        const int nin = left < kUpElems ? (int)left : kUpElems;
+#pragma unroll
+        for (int u = 0; u < kUpElems; ++u) acc[u] = u < nin ? to_d(wk[e0 + u * stride]) : make_double2(0.0, 0.0);
         int i = 0;
         for (; i + 4 <= nv; i += 4) {
-            C b[4];
+            C b[4][kUpElems];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) b[q] = __ldg(Vk + (size_t)(i + q) * vstr + e);
+            for (int q = 0; q < 4; ++q)
+#pragma unroll
+                for (int u = 0; u < kUpElems; ++u)
+                    b[q][u] = u < nin ? __ldg(Vk + (size_t)(i + q) * vstr + e0 + u * stride) : czero<C>();
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
-                const double2 bb = to_d(b[q]), h = cs[i + q];
-                v.x -= h.x * bb.x - h.y * bb.y;
-                v.y -= h.x * bb.y + h.y * bb.x;
+                const double2 h = cs[i + q];
+#pragma unroll
+                for (int u = 0; u < kUpElems; ++u) {
+                    const double2 bb = to_d(b[q][u]);
+                    acc[u].x -= h.x * bb.x - h.y * bb.y;
+                    acc[u].y -= h.x * bb.y + h.y * bb.x;
+                }
             }
         }
         for (; i < nv; ++i) {
-            const double2 bb = to_d(__ldg(Vk + (size_t)i * vstr + e)), h = cs[i];
-            v.x -= h.x * bb.x - h.y * bb.y;
-            v.y -= h.x * bb.y + h.y * bb.x;
+            const double2 h = cs[i];
+#pragma unroll
+            for (int u = 0; u < kUpElems; ++u) {
+                const double2 bb = u < nin ? to_d(__ldg(Vk + (size_t)i * vstr + e0 + u * stride)) : make_double2(0.0, 0.0);
+                acc[u].x -= h.x * bb.x - h.y * bb.y;
+                acc[u].y -= h.x * bb.y + h.y * bb.x;
+            }
         }
-        wk[e] = from_d<C>(make_double2(f * v.x, f * v.y));
+#pragma unroll
+        for (int u = 0; u < kUpElems; ++u)
+            if (u < nin) wk[e0 + u * stride] = from_d<C>(make_double2(f * acc[u].x, f * acc[u].y));
     }
 }
 
@@ -441,12 +475,19 @@ unsigned gs_blocks(long long n) {
     return (unsigned)std::max<long long>(1, std::min<long long>((n + kGsThreads - 1) / kGsThreads, kGsBlocks));
 }
 
+// blocks of a kernel whose threads take `per` elements per round: about two
+// rounds per thread, at least one CTA per SM where the vector allows
+unsigned gs_blocks_per(long long n, int per) {
+    const long long b = (n + (long long)kGsThreads * per * 2 - 1) / ((long long)kGsThreads * per * 2);
+    return (unsigned)std::max<long long>(1, std::min<long long>(std::max<long long>(b, 148), kGsBlocks));
+}
+
 template <typename C> C *basis(GmresWork<C> &gw, int i) { return gw.V + (size_t)i * gw.n * gw.nrhs; }
 
 // h[k * (nv + 1) + i] = V_i[k]^H w[k] for i < nv and ||w[k]||^2 at i = nv (device)
 template <typename C> void multidot(GmresWork<C> &gw, int nv, const C *w, double2 *h, cudaStream_t s) {
     const size_t rstr = gw.n, vstr = (size_t)gw.n * gw.nrhs;
-    const unsigned nb = gs_blocks(gw.n);
+    const unsigned nb = std::min<unsigned>(gs_blocks(gw.n), gs_blocks_per(gw.n, kMdElems));
     count_launches(2);
     launch_dep(k_multidot<C>, dim3(nb, std::max(1, (nv + kGsChunk - 1) / kGsChunk), gw.nrhs), dim3(kGsThreads), 0, s,
                gw.n, nv, nv + 1, (const C *)gw.V, vstr, rstr, w, gw.part);
@@ -520,7 +561,8 @@ tdda_status arnoldi_step(GmresWork<C> &gw, int j, OpFn op_fn, std::vector<std::v
         }
         TDDA_CUDA_TRY(cudaMemcpyAsync(gw.coef, coef.data(), sizeof(double2) * coef.size(), cudaMemcpyHostToDevice, s));
         count_launches(1);
-        launch_dep(k_gs_update_scale<C>, dim3(gs_blocks(gw.n), 1, nr), dim3(kGsThreads), sizeof(double2) * (nv + 1), s,
+        launch_dep(k_gs_update_scale<C>, dim3(gs_blocks_per(gw.n, kUpElems), 1, nr), dim3(kGsThreads),
+                   sizeof(double2) * (nv + 1), s,
                    gw.n, nv, (const C *)gw.V, vstr, rstr, (const double2 *)gw.coef, w);
     }
     return TDDA_OK;
