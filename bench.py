@@ -91,20 +91,20 @@ def parse():
                          "(the case the kernel profiles capture); prints per-pass times")
     ap.add_argument("--profile-gmres", type=int, default=0, metavar="K",
                     help="profile case of the GMRES-DR kernels: one mixed-precision solve of the x-polarised "
-                         "RHS on the 64x64x16 periodic structure (period 64 d, |m|,|n| <= 50), capped at K "
-                         "inner operator applications; prints the solve record")
+                         "RHS of the benchmark structure, capped at K inner operator applications; prints the "
+                         "solve record")
     return ap.parse_args()
 
 
 def run_profile_gmres(k, sici):
-    """A short GMRES-DR solve on a quarter-size periodic cell (the case the
-    Gram-Schmidt kernel profiles capture: same kernels, same basis length per
-    dipole, 3 * 64 * 64 * 16 unknowns per vector)."""
+    """One GMRES-DR solve of the benchmark structure cut off after k inner
+    operator applications (the case the Gram-Schmidt kernel profiles capture:
+    1.57 M complex64 unknowns per basis vector, a basis of up to 61 vectors)."""
     import torch
 
     from dda_model import DDAModel
 
-    w = dict(WORKLOAD, nx=64, ny=64, nz=16, period=64)
+    w = workload()
     m = DDAModel(**model_kwargs(w, sici), precision="mixed")
     m.setDensities(design(w))
     m.setSolver("pgmres", **SOLVER)
@@ -115,7 +115,9 @@ def run_profile_gmres(k, sici):
     t = time.perf_counter()
     info = m.solve_batch_device(B.data_ptr(), X.data_ptr(), 1, True, k, w["tol"], s.cuda_stream)[0]
     torch.cuda.synchronize()
-    print(json.dumps(dict(grid=[64, 64, 16], M=w["M"], seconds=time.perf_counter() - t, **info)))
+    dt = time.perf_counter() - t
+    print(json.dumps(dict(grid=[w["nx"], w["ny"], w["nz"]], M=w["M"], seconds=dt,
+                          ms_per_step=1e3 * dt / max(1, info["iterations"]), **info)))
     return 0
 
 

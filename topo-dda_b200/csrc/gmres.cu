@@ -43,16 +43,93 @@ template <int NV> __device__ __forceinline__ void block_sum_v(double2 (&v)[NV], 
         }
 }
 
+// The two streaming Gram-Schmidt kernels move 16-byte packs: two complex64
+// elements (float4) or one complex128 element.  Vectors whose length or
+// starts are not 16-byte multiples take the element-wise variants.
+template <typename C> struct Pack;
+template <> struct Pack<float2> {
+    using T = float4;
+    static constexpr int E = 2;
+    __device__ static T zero() { return make_float4(0.f, 0.f, 0.f, 0.f); }
+    __device__ static double2 get(const T &p, int i) {
+        return i == 0 ? make_double2(p.x, p.y) : make_double2(p.z, p.w);
+    }
+    __device__ static T make(const double2 (&d)[2]) {
+        return make_float4((float)d[0].x, (float)d[0].y, (float)d[1].x, (float)d[1].y);
+    }
+};
+template <> struct Pack<double2> {
+    using T = double2;
+    static constexpr int E = 1;
+    __device__ static T zero() { return make_double2(0.0, 0.0); }
+    __device__ static double2 get(const T &p, int) { return p; }
+    __device__ static T make(const double2 (&d)[1]) { return d[0]; }
+};
+
 // part[(k * no + i) * gridDim.x + blk] = this block's share of conj(V_i[k]) . w[k]
 // for i < nv; with no = nv + 1 the CTAs of the first chunk also sum ||w[k]||^2
-// into entry i = nv.  A thread takes kMdElems elements per round and issues
-// the loads of all of them (kGsChunk basis vectors each) before using any.
-constexpr int kMdElems = 2;
+// into entry i = nv.  Lengths and strides in packs.  A thread takes kMdPacks
+// packs per round and issues the loads of all of them (kGsChunk basis vectors
+// each, 16 x 16 bytes) before using any: on B200 at 1.57 M complex64 elements
+// this streams 5.1 TB/s against 4.5 TB/s for one element per thread.
+constexpr int kMdPacks = 2;
 
 template <typename C>
-__global__ void __launch_bounds__(kGsThreads) k_multidot(long long n, int nv, int no, const C *__restrict__ V,
-                                                         size_t vstr, size_t rstr, const C *__restrict__ w,
+__global__ void __launch_bounds__(kGsThreads) k_multidot(long long np, int nv, int no,
+                                                         const typename Pack<C>::T *__restrict__ V, size_t vstr,
+                                                         size_t rstr, const typename Pack<C>::T *__restrict__ w,
                                                          double2 *__restrict__ part) {
+    using PK = Pack<C>;
+    using PT = typename PK::T;
+    pdl_wait();
+    __shared__ double2 sm[(kGsChunk + 1) * (kGsThreads / 32)];
+    const int k = blockIdx.z, i0 = blockIdx.y * kGsChunk;
+    const int nb = min(kGsChunk, nv - i0);
+    const bool norm = no > nv && blockIdx.y == 0;
+    double2 acc[kGsChunk + 1];
+#pragma unroll
+    for (int q = 0; q <= kGsChunk; ++q) acc[q] = make_double2(0.0, 0.0);
+    const PT *wk = w + (size_t)k * rstr;
+    const PT *Vk = V + (size_t)k * rstr + (size_t)i0 * vstr;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long p0 = (long long)blockIdx.x * blockDim.x + threadIdx.x; p0 < np; p0 += kMdPacks * stride) {
+        PT wv[kMdPacks], v[kMdPacks][kGsChunk];
+#pragma unroll
+        for (int u = 0; u < kMdPacks; ++u) {
+            const long long p = p0 + u * stride;
+            const bool in = p < np;
+            wv[u] = in ? __ldg(wk + p) : PK::zero();
+#pragma unroll
+            for (int q = 0; q < kGsChunk; ++q) v[u][q] = (in && q < nb) ? __ldg(Vk + (size_t)q * vstr + p) : PK::zero();
+        }
+#pragma unroll
+        for (int u = 0; u < kMdPacks; ++u)
+#pragma unroll
+            for (int e = 0; e < PK::E; ++e) {
+                const double2 wd = PK::get(wv[u], e);
+#pragma unroll
+                for (int q = 0; q < kGsChunk; ++q) {
+                    const double2 d = cdot1(PK::get(v[u][q], e), wd);
+                    acc[q].x += d.x;
+                    acc[q].y += d.y;
+                }
+                if (norm) acc[kGsChunk].x += wd.x * wd.x + wd.y * wd.y;
+            }
+    }
+    block_sum_v<kGsChunk + 1>(acc, sm);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int q = 0; q < kGsChunk; ++q)
+            if (q < nb) part[((size_t)k * no + i0 + q) * gridDim.x + blockIdx.x] = acc[q];
+        if (norm) part[((size_t)k * no + nv) * gridDim.x + blockIdx.x] = acc[kGsChunk];
+    }
+}
+
+// The same sums element by element (any length and alignment).
+template <typename C>
+__global__ void __launch_bounds__(kGsThreads) k_multidot_e(long long n, int nv, int no, const C *__restrict__ V,
+                                                           size_t vstr, size_t rstr, const C *__restrict__ w,
+                                                           double2 *__restrict__ part) {
     pdl_wait();
     __shared__ double2 sm[(kGsChunk + 1) * (kGsThreads / 32)];
     const int k = blockIdx.z, i0 = blockIdx.y * kGsChunk;
@@ -63,46 +140,90 @@ __global__ void __launch_bounds__(kGsThreads) k_multidot(long long n, int nv, in
     for (int q = 0; q <= kGsChunk; ++q) acc[q] = make_double2(0.0, 0.0);
     const C *wk = w + (size_t)k * rstr;
     const C *Vk = V + (size_t)k * rstr + (size_t)i0 * vstr;
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long e0 = (long long)blockIdx.x * blockDim.x + threadIdx.x; e0 < n; e0 += kMdElems * stride) {
-        C wv[kMdElems], v[kMdElems][kGsChunk];
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        const double2 wd = to_d(__ldg(wk + e));
+        C v[kGsChunk];
 #pragma unroll
-        for (int u = 0; u < kMdElems; ++u) {
-            const long long e = e0 + u * stride;
-            const bool in = e < n;
-            wv[u] = in ? __ldg(wk + e) : czero<C>();
+        for (int q = 0; q < kGsChunk; ++q) v[q] = q < nb ? __ldg(Vk + (size_t)q * vstr + e) : czero<C>();
 #pragma unroll
-            for (int q = 0; q < kGsChunk; ++q) v[u][q] = (in && q < nb) ? __ldg(Vk + (size_t)q * vstr + e) : czero<C>();
+        for (int q = 0; q < kGsChunk; ++q) {
+            const double2 d = cdot1(to_d(v[q]), wd);
+            acc[q].x += d.x;
+            acc[q].y += d.y;
         }
-#pragma unroll
-        for (int u = 0; u < kMdElems; ++u) {
-            const double2 wd = to_d(wv[u]);
-#pragma unroll
-            for (int q = 0; q < kGsChunk; ++q) {
-                const double2 d = cdot1(to_d(v[u][q]), wd);
-                acc[q].x += d.x;
-                acc[q].y += d.y;
-            }
-            if (norm) acc[kGsChunk].x += wd.x * wd.x + wd.y * wd.y;
-        }
+        if (norm) acc[kGsChunk].x += wd.x * wd.x + wd.y * wd.y;
     }
     block_sum_v<kGsChunk + 1>(acc, sm);
     if (threadIdx.x == 0) {
-        for (int q = 0; q < nb; ++q) part[((size_t)k * no + i0 + q) * gridDim.x + blockIdx.x] = acc[q];
+#pragma unroll
+        for (int q = 0; q < kGsChunk; ++q)
+            if (q < nb) part[((size_t)k * no + i0 + q) * gridDim.x + blockIdx.x] = acc[q];
         if (norm) part[((size_t)k * no + nv) * gridDim.x + blockIdx.x] = acc[kGsChunk];
     }
 }
 
 // out[k] = (w[k] - sum_{i < nv} c[k][i] V_i[k]) * c[k][nv].x: one Gram-Schmidt
-// update and the normalisation in one pass (c: device, rows of nv + 1).  A
-// thread updates kUpElems elements at once and issues their loads of four
-// basis vectors together (16 loads in flight per thread).
-constexpr int kUpElems = 4;
-
+// update and the normalisation in one pass (c: device, rows of nv + 1).
+// Lengths and strides in packs; one pack per thread, the loads of four basis
+// vectors issued together, 16 CTAs per SM.
 template <typename C>
-__global__ void __launch_bounds__(kGsThreads) k_gs_update_scale(long long n, int nv, const C *__restrict__ V,
+__global__ void __launch_bounds__(kGsThreads) k_gs_update_scale(long long np, int nv,
+                                                                const typename Pack<C>::T *__restrict__ V,
                                                                 size_t vstr, size_t rstr,
-                                                                const double2 *__restrict__ c, C *__restrict__ w) {
+                                                                const double2 *__restrict__ c,
+                                                                typename Pack<C>::T *__restrict__ w) {
+    using PK = Pack<C>;
+    using PT = typename PK::T;
+    pdl_wait();
+    extern __shared__ double2 cs[];
+    const int k = blockIdx.z;
+    for (int i = threadIdx.x; i <= nv; i += blockDim.x) cs[i] = c[(size_t)k * (nv + 1) + i];
+    __syncthreads();
+    const double f = cs[nv].x;
+    PT *wk = w + (size_t)k * rstr;
+    const PT *Vk = V + (size_t)k * rstr;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < np; p += (long long)gridDim.x * blockDim.x) {
+        double2 acc[PK::E];
+        const PT w0 = wk[p];
+#pragma unroll
+        for (int e = 0; e < PK::E; ++e) acc[e] = PK::get(w0, e);
+        int i = 0;
+        for (; i + 4 <= nv; i += 4) {
+            PT b[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) b[q] = __ldg(Vk + (size_t)(i + q) * vstr + p);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const double2 h = cs[i + q];
+#pragma unroll
+                for (int e = 0; e < PK::E; ++e) {
+                    const double2 bb = PK::get(b[q], e);
+                    acc[e].x -= h.x * bb.x - h.y * bb.y;
+                    acc[e].y -= h.x * bb.y + h.y * bb.x;
+                }
+            }
+        }
+        for (; i < nv; ++i) {
+            const double2 h = cs[i];
+            const PT b = __ldg(Vk + (size_t)i * vstr + p);
+#pragma unroll
+            for (int e = 0; e < PK::E; ++e) {
+                const double2 bb = PK::get(b, e);
+                acc[e].x -= h.x * bb.x - h.y * bb.y;
+                acc[e].y -= h.x * bb.y + h.y * bb.x;
+            }
+        }
+#pragma unroll
+        for (int e = 0; e < PK::E; ++e) acc[e] = make_double2(f * acc[e].x, f * acc[e].y);
+        wk[p] = PK::make(acc);
+    }
+}
+
+// The same update element by element (any length and alignment).
+template <typename C>
+__global__ void __launch_bounds__(kGsThreads) k_gs_update_scale_e(long long n, int nv, const C *__restrict__ V,
+                                                                  size_t vstr, size_t rstr,
+                                                                  const double2 *__restrict__ c, C *__restrict__ w) {
     pdl_wait();
     extern __shared__ double2 cs[];
     const int k = blockIdx.z;
@@ -111,45 +232,26 @@ __global__ void __launch_bounds__(kGsThreads) k_gs_update_scale(long long n, int
     const double f = cs[nv].x;
     C *wk = w + (size_t)k * rstr;
     const C *Vk = V + (size_t)k * rstr;
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long e0 = (long long)blockIdx.x * blockDim.x + threadIdx.x; e0 < n; e0 += kUpElems * stride) {
-        double2 acc[kUpElems];
-        // elements u < nin of this round lie inside the vector
-        const long long left = (n - e0 + stride - 1) / stride;
-        const int nin = left < kUpElems ? (int)left : kUpElems;
-#pragma unroll
-        for (int u = 0; u < kUpElems; ++u) acc[u] = u < nin ? to_d(wk[e0 + u * stride]) : make_double2(0.0, 0.0);
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        double2 acc = to_d(wk[e]);
         int i = 0;
         for (; i + 4 <= nv; i += 4) {
-            C b[4][kUpElems];
+            C b[4];
 #pragma unroll
-            for (int q = 0; q < 4; ++q)
-#pragma unroll
-                for (int u = 0; u < kUpElems; ++u)
-                    b[q][u] = u < nin ? __ldg(Vk + (size_t)(i + q) * vstr + e0 + u * stride) : czero<C>();
+            for (int q = 0; q < 4; ++q) b[q] = __ldg(Vk + (size_t)(i + q) * vstr + e);
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
-                const double2 h = cs[i + q];
-#pragma unroll
-                for (int u = 0; u < kUpElems; ++u) {
-                    const double2 bb = to_d(b[q][u]);
-                    acc[u].x -= h.x * bb.x - h.y * bb.y;
-                    acc[u].y -= h.x * bb.y + h.y * bb.x;
-                }
+                const double2 h = cs[i + q], bb = to_d(b[q]);
+                acc.x -= h.x * bb.x - h.y * bb.y;
+                acc.y -= h.x * bb.y + h.y * bb.x;
             }
         }
         for (; i < nv; ++i) {
-            const double2 h = cs[i];
-#pragma unroll
-            for (int u = 0; u < kUpElems; ++u) {
-                const double2 bb = u < nin ? to_d(__ldg(Vk + (size_t)i * vstr + e0 + u * stride)) : make_double2(0.0, 0.0);
-                acc[u].x -= h.x * bb.x - h.y * bb.y;
-                acc[u].y -= h.x * bb.y + h.y * bb.x;
-            }
+            const double2 h = cs[i], bb = to_d(__ldg(Vk + (size_t)i * vstr + e));
+            acc.x -= h.x * bb.x - h.y * bb.y;
+            acc.y -= h.x * bb.y + h.y * bb.x;
         }
-#pragma unroll
-        for (int u = 0; u < kUpElems; ++u)
-            if (u < nin) wk[e0 + u * stride] = from_d<C>(make_double2(f * acc[u].x, f * acc[u].y));
+        wk[e] = from_d<C>(make_double2(f * acc.x, f * acc.y));
     }
 }
 
@@ -319,6 +421,7 @@ template <typename C> tdda_status GmresWork<C>::init(long long n3, int nrhs_, in
     TDDA_CUDA_TRY(cudaMalloc(&P, sizeof(double2) * (size_t)nrhs * (restart + 1) * (deflate + 1)));
     TDDA_CUDA_TRY(cudaMalloc(&nrm, sizeof(double) * 2 * nrhs));
     TDDA_CUDA_TRY(cudaMallocHost(&h_host, sizeof(double2) * (2 * (size_t)nrhs * (restart + 1) + nrhs)));
+    TDDA_CUDA_TRY(cudaMallocHost(&c_host, sizeof(double2) * (size_t)nrhs * (restart + 1)));
     return TDDA_OK;
 }
 
@@ -326,10 +429,11 @@ template <typename C> void GmresWork<C>::release() {
     cudaFree(V); cudaFree(V2); cudaFree(U); cudaFree(W); cudaFree(Y);
     cudaFree(part); cudaFree(h); cudaFree(coef); cudaFree(P); cudaFree(nrm);
     cudaFreeHost(h_host);
+    cudaFreeHost(c_host);
     V = V2 = U = W = Y = nullptr;
     part = h = coef = P = nullptr;
     nrm = nullptr;
-    h_host = nullptr;
+    h_host = c_host = nullptr;
     nrhs = 0;
 }
 
@@ -475,25 +579,55 @@ unsigned gs_blocks(long long n) {
     return (unsigned)std::max<long long>(1, std::min<long long>((n + kGsThreads - 1) / kGsThreads, kGsBlocks));
 }
 
-// blocks of a kernel whose threads take `per` elements per round: about two
-// rounds per thread, at least one CTA per SM where the vector allows
-unsigned gs_blocks_per(long long n, int per) {
-    const long long b = (n + (long long)kGsThreads * per * 2 - 1) / ((long long)kGsThreads * per * 2);
-    return (unsigned)std::max<long long>(1, std::min<long long>(std::max<long long>(b, 148), kGsBlocks));
+// whether the basis and w[k] can be read in 16-byte packs
+template <typename C> bool packed(const GmresWork<C> &gw, const void *w) {
+    constexpr int E = Pack<C>::E;
+    return gw.n % E == 0 && ((uintptr_t)gw.V & 15) == 0 && ((uintptr_t)w & 15) == 0;
 }
 
 template <typename C> C *basis(GmresWork<C> &gw, int i) { return gw.V + (size_t)i * gw.n * gw.nrhs; }
 
 // h[k * (nv + 1) + i] = V_i[k]^H w[k] for i < nv and ||w[k]||^2 at i = nv (device)
 template <typename C> void multidot(GmresWork<C> &gw, int nv, const C *w, double2 *h, cudaStream_t s) {
+    using PT = typename Pack<C>::T;
+    constexpr int E = Pack<C>::E;
     const size_t rstr = gw.n, vstr = (size_t)gw.n * gw.nrhs;
-    const unsigned nb = std::min<unsigned>(gs_blocks(gw.n), gs_blocks_per(gw.n, kMdElems));
+    const unsigned nch = (unsigned)std::max(1, (nv + kGsChunk - 1) / kGsChunk);
+    unsigned nb;
     count_launches(2);
-    launch_dep(k_multidot<C>, dim3(nb, std::max(1, (nv + kGsChunk - 1) / kGsChunk), gw.nrhs), dim3(kGsThreads), 0, s,
-               gw.n, nv, nv + 1, (const C *)gw.V, vstr, rstr, w, gw.part);
+    if (packed(gw, w)) {
+        const long long np = gw.n / E;
+        nb = (unsigned)std::max<long long>(
+            1, std::min<long long>((np + kGsThreads * kMdPacks - 1) / (kGsThreads * kMdPacks), kGsBlocks));
+        launch_dep(k_multidot<C>, dim3(nb, nch, gw.nrhs), dim3(kGsThreads), 0, s, np, nv, nv + 1,
+                   (const PT *)gw.V, vstr / E, rstr / E, (const PT *)w, gw.part);
+    } else {
+        nb = gs_blocks(gw.n);
+        launch_dep(k_multidot_e<C>, dim3(nb, nch, gw.nrhs), dim3(kGsThreads), 0, s, gw.n, nv, nv + 1,
+                   (const C *)gw.V, vstr, rstr, w, gw.part);
+    }
     const int nout = gw.nrhs * (nv + 1);
     launch_dep(k_sum_parts, dim3((nout + 7) / 8), dim3(256), 0, s, nout, (int)nb, (const double2 *)gw.part, h,
                (double *)nullptr, (double *)nullptr);
+}
+
+// w[k] = (w[k] - V[0..nv)[k] c[k]) * c[k][nv].x (c: device, rows of nv + 1)
+template <typename C> void gs_update_scale(GmresWork<C> &gw, int nv, const double2 *c, C *w, cudaStream_t s) {
+    using PT = typename Pack<C>::T;
+    constexpr int E = Pack<C>::E;
+    const size_t rstr = gw.n, vstr = (size_t)gw.n * gw.nrhs;
+    const size_t smem = sizeof(double2) * (nv + 1);
+    count_launches(1);
+    if (packed(gw, w)) {
+        const long long np = gw.n / E;
+        const unsigned nb = (unsigned)std::max<long long>(1, std::min<long long>((np + kGsThreads - 1) / kGsThreads,
+                                                                                 148 * 16));
+        launch_dep(k_gs_update_scale<C>, dim3(nb, 1, gw.nrhs), dim3(kGsThreads), smem, s, np, nv, (const PT *)gw.V,
+                   vstr / E, rstr / E, c, (PT *)w);
+    } else {
+        launch_dep(k_gs_update_scale_e<C>, dim3(gs_blocks(gw.n), 1, gw.nrhs), dim3(kGsThreads), smem, s, gw.n, nv,
+                   (const C *)gw.V, vstr, rstr, c, w);
+    }
 }
 
 // w[k] -= V[0..nv)[k] h[k]; with norms: nrm[k] = ||w[k]||, nrm[nrhs + k] = 1 / nrm[k]
@@ -529,9 +663,8 @@ tdda_status arnoldi_step(GmresWork<C> &gw, int j, OpFn op_fn, std::vector<std::v
     C *w = basis(gw, j + 1);
     tdda_status st = op_fn(basis(gw, j), w);
     if (st != TDDA_OK) return st;
-    const size_t rstr = gw.n, vstr = (size_t)gw.n * nr;
     double2 *hh = gw.h_host;
-    std::vector<double2> coef((size_t)nr * (nv + 1));
+    double2 *coef = gw.c_host;
     for (int k = 0; k < nr; ++k) Hcol[k].assign(nv + 1, cplx(0.0));
     bool final = false;
     for (int pass = 0; pass < 2 && !final; ++pass) {
@@ -559,11 +692,8 @@ tdda_status arnoldi_step(GmresWork<C> &gw, int j, OpFn op_fn, std::vector<std::v
             coef[(size_t)k * (nv + 1) + nv] = make_double2(final ? (nrm > 0.0 ? 1.0 / nrm : 0.0) : 1.0, 0.0);
             if (final) Hcol[k][nv] = cplx(nrm, 0.0);
         }
-        TDDA_CUDA_TRY(cudaMemcpyAsync(gw.coef, coef.data(), sizeof(double2) * coef.size(), cudaMemcpyHostToDevice, s));
-        count_launches(1);
-        launch_dep(k_gs_update_scale<C>, dim3(gs_blocks_per(gw.n, kUpElems), 1, nr), dim3(kGsThreads),
-                   sizeof(double2) * (nv + 1), s,
-                   gw.n, nv, (const C *)gw.V, vstr, rstr, (const double2 *)gw.coef, w);
+        TDDA_CUDA_TRY(cudaMemcpyAsync(gw.coef, coef, sizeof(double2) * (size_t)nr * (nv + 1), cudaMemcpyHostToDevice, s));
+        gs_update_scale(gw, nv, (const double2 *)gw.coef, w, s);
     }
     return TDDA_OK;
 }

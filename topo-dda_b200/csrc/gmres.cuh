@@ -40,6 +40,7 @@ template <typename C> struct GmresWork {
     double2 *coef = nullptr;    // device [nrhs][restart + 1] combination weights
     double2 *P = nullptr;       // device [nrhs][restart + 1][deflate + 1] restart combinations
     double2 *h_host = nullptr;  // pinned mirror of h, nrm
+    double2 *c_host = nullptr;  // pinned staging of coef
     tdda_status init(long long n3, int nrhs, int restart, int degree, int deflate);
     void release();
     size_t bytes() const;
