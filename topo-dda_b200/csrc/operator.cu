@@ -68,7 +68,8 @@ template <int NQ> __device__ __forceinline__ void block_sum(double2 (&v)[NQ]) {
 // Every block contributes NQ complex sums; the last block to finish adds the
 // per-block partials in block order and calls fin(rhs, totals) on thread 0.
 // The partials of one RHS take nblk * NQ entries: the scratch holds
-// max(3 nx, UPD_BLOCKS) * kMaxNQ per RHS (pass 3 runs nx * 3 blocks per RHS,
+// max(6 nx, UPD_BLOCKS) * kMaxNQ per RHS (pass 3 runs nx * 3 blocks per RHS,
+// 2 nx * 3 in the complex128 cluster form,
 // the vector kernels UPD_BLOCKS), and no reduction uses more than kMaxNQ sums.
 constexpr int kMaxNQ = 4;
 template <int NQ, class Fin>
@@ -650,6 +651,7 @@ static bool launch_inv_fast(const ConvGeom &g, dim3 grid, const C *T, const C *t
 
 }  // namespace tdda
 #include "slab_reg.cuh"
+#include "slab_cluster.cuh"
 namespace tdda {
 
 template <typename C, class Epi>
@@ -1211,6 +1213,21 @@ template <typename C> static void set_smem_attrs(int yz, int x) {
         TDDA_YZ_REG_PAIRS(TDDA_ATTR_REG)
 #undef TDDA_ATTR_REG
     }
+    if constexpr (sizeof(C) == 16) {
+#define TDDA_ATTR_CL(a, b)                                                                                           \
+    cudaFuncSetAttribute(k_fwd_zy_cl<C, a, b, ProLoad<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, ClGeom<a, b>::SMEM); \
+    cudaFuncSetAttribute(k_fwd_zy_cl<C, a, b, ProP<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, ClGeom<a, b>::SMEM);    \
+    cudaFuncSetAttribute(k_fwd_zy_cl<C, a, b, ProT<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, ClGeom<a, b>::SMEM);    \
+    cudaFuncSetAttribute(k_fwd_zy_cl<C, a, b, ProPF<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, ClGeom<a, b>::SMEM);   \
+    cudaFuncSetAttribute(k_inv_yz_cl<C, a, b, EpiAtF<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, ClGeom<a, b>::SMEM);  \
+    cudaFuncSetAttribute(k_inv_yz_cl<C, a, b, EpiMatvec<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, ClGeom<a, b>::SMEM); \
+    cudaFuncSetAttribute(k_inv_yz_cl<C, a, b, EpiPoly<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, ClGeom<a, b>::SMEM); \
+    cudaFuncSetAttribute(k_inv_yz_cl<C, a, b, EpiInit<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, ClGeom<a, b>::SMEM); \
+    cudaFuncSetAttribute(k_inv_yz_cl<C, a, b, EpiAp<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, ClGeom<a, b>::SMEM);   \
+    cudaFuncSetAttribute(k_inv_yz_cl<C, a, b, EpiAt<C>>, cudaFuncAttributeMaxDynamicSharedMemorySize, ClGeom<a, b>::SMEM);
+        TDDA_YZ_CL_PAIRS(TDDA_ATTR_CL)
+#undef TDDA_ATTR_CL
+    }
     cudaGetLastError();  // a refused opt-in shows up at launch time, not here
 }
 
@@ -1266,6 +1283,9 @@ static bool plan_geom(int nx, int ny, int nz, int nrhs, int esize, ConvGeom &g, 
         g.smem_ir = slab_reg_smem(ny, g.Lz, g.Ly, false, esize);
         g.reg_yz = (g.smem_fr <= kSmemFast && g.smem_ir <= kSmemFast) ? 1 : 0;
     }
+    // complex128: the slab split over a two-CTA cluster
+    g.cl_yz = (esize == 16 && 2 * ny == g.Ly && 2 * nz == g.Lz && cl_yz_pair(g.Lz, g.Ly) &&
+               cl_smem(g.Lz, g.Ly) <= kSmemFast) ? 1 : 0;
     // compile-time-length pass 2: two ping-pong buffers, at most ~100 KB so
     // that two CTAs share an SM; runs of >= 64 bytes along kz
     g.fast_x = fast_x_length(g.Lx) ? 1 : 0;
@@ -1326,7 +1346,7 @@ template <typename C> tdda_status ConvOperator<C>::init(int nx, int ny, int nz, 
     TDDA_CUDA_TRY(cudaMalloc(&tw, sizeof(C) * g.Lmax));
     TDDA_CUDA_TRY(cudaMemcpy(tw, h.data(), sizeof(C) * g.Lmax, cudaMemcpyHostToDevice));
     TDDA_CUDA_TRY(cudaMalloc(&T, sizeof(C) * (size_t)nrhs_cap * 3 * g.tcomp));
-    partial_cap = std::max(3 * nx, UPD_BLOCKS) * kMaxNQ;
+    partial_cap = std::max(6 * nx, UPD_BLOCKS) * kMaxNQ;
     TDDA_CUDA_TRY(cudaMalloc(&partials, sizeof(double2) * (size_t)partial_cap * nrhs_cap));
     TDDA_CUDA_TRY(cudaMalloc(&counters, sizeof(unsigned) * (size_t)nrhs_cap));
     TDDA_CUDA_TRY(cudaMemset(counters, 0, sizeof(unsigned) * (size_t)nrhs_cap));
@@ -1337,7 +1357,7 @@ size_t conv_workspace_bytes(int nx, int ny, int nz, int nrhs_cap, int esize) {
     ConvGeom g;
     std::string why;
     if (!plan_geom(nx, ny, nz, 1, esize, g, why)) return 0;
-    const size_t partial_cap = (size_t)std::max(3 * nx, UPD_BLOCKS) * kMaxNQ;
+    const size_t partial_cap = (size_t)std::max(6 * nx, UPD_BLOCKS) * kMaxNQ;
     return (size_t)esize * g.Lmax + (size_t)esize * nrhs_cap * 3 * g.tcomp + sizeof(double2) * partial_cap * nrhs_cap +
            sizeof(unsigned) * nrhs_cap;
 }
@@ -1363,7 +1383,7 @@ static tdda_status run_conv(ConvOperator<C> &op, const ConvGeom &g, int nrhs, co
                             const Epi &epi, const SolverState *st, cudaStream_t s) {
     dim3 g13(g.nx, 3, nrhs);
     count_launches(1);
-    if (!launch_fwd_reg<C, Pro>(g, g13, op.T, op.tw, pro, s) &&
+    if (!launch_fwd_reg<C, Pro>(g, g13, op.T, op.tw, pro, s) && !launch_fwd_cl<C, Pro>(g, g13, op.T, op.tw, pro, s) &&
         !(g.fast_yz && launch_fwd_fast<C, Pro>(g, g13, op.T, op.tw, pro, s)))
         launch_dep((k_fwd_zy<C, Pro>), g13, dim3(NT), g.smem_yz, s, g, op.T, op.tw, pro);
     dim3 g2(g.Ly, g.CKx > 0 ? g.Lz / g.CKx : 1, 1);
@@ -1372,7 +1392,7 @@ static tdda_status run_conv(ConvOperator<C> &op, const ConvGeom &g, int nrhs, co
         !(g.fast_x && launch_xconv_fast<C>(g, op.T, op.ahat, op.ahat_rhs, op.tw, nrhs, st, s)))
         launch_dep(k_xconv<C>, g2, dim3(NT), g.smem_x, s, g, op.T, op.ahat, op.ahat_rhs, op.tw, nrhs, st);
     count_launches(1);
-    if (!launch_inv_reg<C, Epi>(g, g13, op.T, op.tw, epi, s) &&
+    if (!launch_inv_reg<C, Epi>(g, g13, op.T, op.tw, epi, s) && !launch_inv_cl<C, Epi>(g, g13, op.T, op.tw, epi, s) &&
         !(g.fast_yz && launch_inv_fast<C, Epi>(g, g13, op.T, op.tw, epi, s)))
         launch_dep((k_inv_yz<C, Epi>), g13, dim3(NT), g.smem_yz, s, g, op.T, op.tw, epi);
     return TDDA_OK;
@@ -1743,6 +1763,7 @@ tdda_status profile_apply(ConvOperator<C> &op, const C *x, C *y, const C *al, in
     ms_pass[0] = timed([&] {
         count_launches(1);
         if (!launch_fwd_reg<C, ProLoad<C>>(g, g13, op.T, op.tw, pro, s) &&
+            !launch_fwd_cl<C, ProLoad<C>>(g, g13, op.T, op.tw, pro, s) &&
             !(g.fast_yz && launch_fwd_fast<C, ProLoad<C>>(g, g13, op.T, op.tw, pro, s)))
             k_fwd_zy<C, ProLoad<C>><<<g13, NT, g.smem_yz, s>>>(g, op.T, op.tw, pro);
     });
@@ -1755,6 +1776,7 @@ tdda_status profile_apply(ConvOperator<C> &op, const C *x, C *y, const C *al, in
     ms_pass[2] = timed([&] {
         count_launches(1);
         if (!launch_inv_reg<C, EpiMatvec<C>>(g, g13, op.T, op.tw, epi, s) &&
+            !launch_inv_cl<C, EpiMatvec<C>>(g, g13, op.T, op.tw, epi, s) &&
             !(g.fast_yz && launch_inv_fast<C, EpiMatvec<C>>(g, g13, op.T, op.tw, epi, s)))
             k_inv_yz<C, EpiMatvec<C>><<<g13, NT, g.smem_yz, s>>>(g, op.T, op.tw, epi);
     });

@@ -98,6 +98,7 @@ struct ConvGeom {
     int smem_yz;        // dynamic SMEM bytes, passes 1 and 3
     int smem_x;         // dynamic SMEM bytes, pass 2
     int fast_yz;        // 1: passes 1 and 3 use the compile-time (Lz, Ly) slab kernels
+    int cl_yz;          // 1: complex128 passes 1 and 3 use the two-CTA cluster slab kernels
     int smem_yz2;       // their dynamic SMEM bytes
     int fast_x;         // 1: pass 2 uses the compile-time-length kernel for Lx
     int CKx2;           // kz chunk of that kernel
