@@ -172,7 +172,7 @@ class ClockSampler:
 
     FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap,utilization.gpu")
 
     def __init__(self, index):
         self.index = index
@@ -214,6 +214,11 @@ class ClockSampler:
                           if len(r) > 4 + i and r[4 + i].lower().startswith("active")})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "samples": len(self.rows), "reasons": reasons}
+
+    def gpu_busy(self):
+        """Mean of nvidia-smi's utilization.gpu (percent of time a kernel ran)."""
+        u = [float(r[8]) for r in self.rows if len(r) > 8 and r[8].replace(".", "").isdigit()]
+        return statistics.mean(u) / 100.0 if u else None
 
 
 def peaks():
@@ -507,7 +512,8 @@ def run_serving(rank=0, world=1, device=None):
     with DDAServer(hbm_budget_bytes=120 * 10**9, workers=4, max_rhs=8, use_graphs=True) as srv:
         for shape in SERVE_SHAPES:   # workspaces allocated before the stream starts
             srv.reserve(shape)
-        rep = run_stream(srv, reqs)
+        with ClockSampler(torch_index(device)) as clk:
+            rep = run_stream(srv, reqs)
         st = srv.stats()
     s = rep.summary()
     log(f"serving (rank {rank}/{world}, {len(reqs)} requests): {s}")
@@ -524,7 +530,14 @@ def run_serving(rank=0, world=1, device=None):
             "converged_rhs": s["converged_rhs"], "rhs": s["rhs"], "max_true_error": s["max_true_error"],
             "batches": st["batches"], "merged_requests": st["merged_requests"],
             "peak_bytes": st["peak_bytes"], "latency": "submit to result, wall clock, includes queueing",
+            "gpu_busy": clk.gpu_busy(), "per_grid": rep.per_shape(),
             "below_capacity": run_serving_light(rank, world, device)}
+
+
+def torch_index(device):
+    import torch
+
+    return torch.device(device).index if device is not None else torch.cuda.current_device()
 
 
 def run_serving_light(rank=0, world=1, device=None, n=256, rate=30.0):

@@ -262,7 +262,10 @@ tdda_status tdda_set_time_limit(tdda_model *m, double seconds);
  * a polynomial of `degree` (1..64; 1 is plain GMRES) in it, built from the
  * harmonic Ritz values of the first residual's Krylov space; a restart keeps
  * the `deflate` (0..restart-1) harmonic Ritz vectors of smallest magnitude
- * (deflated restarting, GMRES-DR).  Inner solves run in complex64 for
+ * (deflated restarting, GMRES-DR).  kind 2: as kind 1, and the inner solve of
+ * each refinement step after the first starts from the deflation space the
+ * previous one ended with, the new residual orthonormalised against it, instead
+ * of from the residual alone (1 <= deflate <= restart - 6).  Inner solves run in complex64 for
  * mixed-precision models.  The solve stops when ||E - A P|| / ||E|| <= tol;
  * max_iter bounds the inner operator applications (tdda_solve_info:
  * iterations = GMRES steps, inner_iterations = operator applications,

@@ -13,13 +13,13 @@ from cases import model_args, rel
 pytestmark = pytest.mark.gpu
 
 
-def _solve(kw, precision, degree, restart, tol, B, max_iter=200000, deflate=0):
+def _solve(kw, precision, degree, restart, tol, B, max_iter=200000, deflate=0, kind="pgmres"):
     import torch
 
     from dda_model import DDAModel
 
     m = DDAModel(**kw, precision=precision)
-    m.setSolver("pgmres", degree=degree, restart=restart, deflate=deflate)
+    m.setSolver(kind, degree=degree, restart=restart, deflate=deflate)
     nrhs = B.shape[0]
     Bd = torch.from_numpy(B).cuda()
     X = torch.zeros_like(Bd)
@@ -102,3 +102,43 @@ def test_deflated_restarts_match_oracle(sici, precision, degree, restart, deflat
         res = np.linalg.norm(B[k] - ora.aproduct_with_alb(X[k])) / np.linalg.norm(B[k])
         assert res <= 1.0001 * tol, (k, res, infos[k])
         assert rel(X[k], np.linalg.solve(A, B[k])) < 1e3 * tol
+
+
+@pytest.mark.parametrize("precision,tol", [("mixed", 1e-8), ("mixed", 1e-11), ("complex128", 1e-13)])
+@pytest.mark.parametrize("shape,M,nrhs,restart,deflate", [((12, 12, 6), 20, 2, 16, 6), ((16, 16, 8), 50, 1, 24, 10)])
+def test_recycled_deflation_space_matches_oracle(sici, precision, tol, shape, M, nrhs, restart, deflate):
+    """Solver kind 2: every refinement step after the first starts its inner
+    solve from the deflation space the previous one ended with (the new
+    residual orthonormalised against it; the cycles then carry the extra
+    directions).  Mixed precision takes several refinement steps, so the
+    carried space is used; the true residual and the dense solve decide."""
+    from oracle.dda_oracle import OracleModel
+
+    nx, ny, nz = shape
+    kw = model_args(nx, ny, nz, sici, MAXm=M, MAXn=M, seed=4)
+    ora = OracleModel(**kw)
+    B = _rhs(ora, nrhs, 8)
+    X, infos = _solve(kw, precision, 1, restart, tol, B, deflate=deflate, kind="gmres-dr-recycle")
+    A = ora.dense_operator() if ora.N <= 1500 else None
+    for k in range(nrhs):
+        i = infos[k]
+        assert i["status"] == "converged", i
+        if precision == "mixed":
+            assert i["refinements"] >= 2, i
+        res = np.linalg.norm(B[k] - ora.aproduct_with_alb(X[k])) / np.linalg.norm(B[k])
+        assert res <= 1.0001 * tol, (k, res, i)
+        # the two residual evaluations differ by round-off (~1e-16 relative to ||B||)
+        assert abs(i["true_error"] - res) <= max(1e-3 * tol, 1e-15), (i["true_error"], res)
+        if A is not None:
+            assert rel(X[k], np.linalg.solve(A, B[k])) < 1e4 * tol
+
+
+def test_recycling_rejects_too_short_cycles(sici):
+    from dda_model import DDAModel
+
+    m = DDAModel(**model_args(8, 8, 4, sici, seed=1))
+    with pytest.raises(RuntimeError):
+        m.setSolver("gmres-dr-recycle", degree=1, restart=10, deflate=6)
+    with pytest.raises(RuntimeError):
+        m.setSolver("gmres-dr-recycle", degree=1, restart=10, deflate=0)
+    m.setSolver("gmres-dr-recycle", degree=1, restart=12, deflate=6)

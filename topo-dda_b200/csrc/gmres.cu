@@ -17,6 +17,9 @@ namespace tdda {
 constexpr int kGsThreads = 256;
 constexpr int kGsBlocks = 148 * 4;
 constexpr int kGsChunk = 8;   // basis vectors per multi-dot CTA
+// directions beyond the residual's that a recycled start may carry (each
+// refinement step that starts from a recycled space adds one)
+constexpr int kMaxAug = 4;
 
 template <int NV> __device__ __forceinline__ void block_sum_v(double2 (&v)[NV], double2 *sm) {
     // sm: NV * (kGsThreads / 32) double2
@@ -118,6 +121,149 @@ __global__ void __launch_bounds__(kGsThreads) k_multidot(long long np, int nv, i
     }
     block_sum_v<kGsChunk + 1>(acc, sm);
     if (threadIdx.x == 0) {
+#pragma unroll
+        for (int q = 0; q < kGsChunk; ++q)
+            if (q < nb) part[((size_t)k * no + i0 + q) * gridDim.x + blockIdx.x] = acc[q];
+        if (norm) part[((size_t)k * no + nv) * gridDim.x + blockIdx.x] = acc[kGsChunk];
+    }
+}
+
+// The same sums with the vectors streamed into shared memory by the bulk-copy
+// engine (cp.async.bulk, global -> shared, completion on an mbarrier): tiles
+// of kBdTile packs of w and of every basis vector of the CTA's chunk, kBdStages
+// tiles in a ring, kBdStages - 1 of them in flight while the threads work on
+// the oldest.  The bytes in flight do not cost registers, so two CTAs per SM
+// keep ~144 KB of loads outstanding.  CTA (x, chunk, rhs) takes the tiles
+// x, x + gridDim.x, ... of its chunk; partials as in k_multidot.  A wait that
+// has not completed after kBdSpin polls marks the CTA's partials NaN (the host
+// rejects non-finite sums) and stops the CTA; every copy issued before has
+// been waited for by then or belongs to the stalled tile.
+constexpr int kBdTile = 256;    // packs per vector per tile (4 KB)
+constexpr int kBdStages = 3;
+constexpr long long kBdSpin = 1ll << 22;
+constexpr size_t kBdSmem = (size_t)kBdStages * (kGsChunk + 1) * kBdTile * 16;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+template <typename C>
+__global__ void __launch_bounds__(kGsThreads, 2) k_multidot_bulk(long long np, int nv, int no,
+                                                                 const typename Pack<C>::T *__restrict__ V,
+                                                                 size_t vstr, size_t rstr,
+                                                                 const typename Pack<C>::T *__restrict__ w,
+                                                                 double2 *__restrict__ part) {
+    using PK = Pack<C>;
+    using PT = typename PK::T;
+    extern __shared__ __align__(128) unsigned char bd_smem[];
+    __shared__ __align__(8) unsigned long long full[kBdStages];
+    __shared__ double2 sm[(kGsChunk + 1) * (kGsThreads / 32)];
+    PT *tiles = reinterpret_cast<PT *>(bd_smem);   // [stage][vector (w last)][kBdTile]
+    const int k = blockIdx.z, i0 = blockIdx.y * kGsChunk;
+    const int nb = min(kGsChunk, nv - i0);
+    const bool norm = no > nv && blockIdx.y == 0;
+    const long long ntiles = (np + kBdTile - 1) / kBdTile;
+    const PT *wk = w + (size_t)k * rstr;
+    const PT *Vk = V + (size_t)k * rstr + (size_t)i0 * vstr;
+    if (threadIdx.x == 0) {
+        for (int st = 0; st < kBdStages; ++st)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&full[st])) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    pdl_wait();
+    // tile t into ring slot st (thread 0)
+    auto issue = [&](long long t, int st) {
+        const long long p0 = t * kBdTile;
+        const uint32_t bytes = (uint32_t)(min((long long)kBdTile, np - p0) * 16);
+        const uint32_t bar = smem_u32(&full[st]);
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes * (nb + 1))
+                     : "memory");
+        PT *slot = tiles + (size_t)st * (kGsChunk + 1) * kBdTile;
+        for (int q = 0; q <= nb; ++q) {
+            const PT *src = (q < nb ? Vk + (size_t)q * vstr : wk) + p0;
+            PT *dst = slot + (size_t)(q < nb ? q : kGsChunk) * kBdTile;
+            asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+                             "r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(bar)
+                         : "memory");
+        }
+    };
+    double2 acc[kGsChunk + 1];
+#pragma unroll
+    for (int q = 0; q <= kGsChunk; ++q) acc[q] = make_double2(0.0, 0.0);
+    const long long t0 = blockIdx.x, dt = gridDim.x;
+    if (threadIdx.x == 0)
+        for (int st = 0; st < kBdStages - 1; ++st)
+            if (t0 + st * dt < ntiles) issue(t0 + st * dt, st);
+    bool stalled = false;
+    long long it = 0;
+    for (long long t = t0; t < ntiles; t += dt, ++it) {
+        const int st = (int)(it % kBdStages);
+        const uint32_t parity = (uint32_t)((it / kBdStages) & 1);
+        if (threadIdx.x == 0) {
+            // the slot refilled here was read in iteration it - 1, which every
+            // thread has left (barrier at the end of the loop)
+            const long long tn = t + (kBdStages - 1) * dt;
+            if (tn < ntiles) {
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                issue(tn, (int)((it + kBdStages - 1) % kBdStages));
+            }
+        }
+        uint32_t ok = 0;
+        for (long long spin = 0; !ok; ++spin) {
+            asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                         " selp.u32 %0, 1, 0, p;\n}"
+                         : "=r"(ok)
+                         : "r"(smem_u32(&full[st])), "r"(parity)
+                         : "memory");
+            if (!ok && spin > kBdSpin) break;
+        }
+        if (!__syncthreads_and((int)ok)) {
+            stalled = true;
+            // let the copies already issued land (bounded) before the CTA ends
+            if (threadIdx.x == 0)
+                for (int a = 0; a < kBdStages - 1; ++a) {
+                    const long long ia = it + a;
+                    if (t + a * dt >= ntiles) break;
+                    const uint32_t par = (uint32_t)((ia / kBdStages) & 1);
+                    uint32_t got = 0;
+                    for (long long spin = 0; !got && spin <= kBdSpin; ++spin)
+                        asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                                     " selp.u32 %0, 1, 0, p;\n}"
+                                     : "=r"(got)
+                                     : "r"(smem_u32(&full[(int)(ia % kBdStages)])), "r"(par)
+                                     : "memory");
+                }
+            __syncthreads();
+            break;
+        }
+        const PT *slot = tiles + (size_t)st * (kGsChunk + 1) * kBdTile;
+        const long long cnt = min((long long)kBdTile, np - t * kBdTile);
+        for (int p = threadIdx.x; p < cnt; p += kGsThreads) {
+            const PT wv = slot[(size_t)kGsChunk * kBdTile + p];
+            PT v[kGsChunk];
+#pragma unroll
+            for (int q = 0; q < kGsChunk; ++q) v[q] = q < nb ? slot[(size_t)q * kBdTile + p] : PK::zero();
+#pragma unroll
+            for (int e = 0; e < PK::E; ++e) {
+                const double2 wd = PK::get(wv, e);
+#pragma unroll
+                for (int q = 0; q < kGsChunk; ++q) {
+                    const double2 d = cdot1(PK::get(v[q], e), wd);
+                    acc[q].x += d.x;
+                    acc[q].y += d.y;
+                }
+                if (norm) acc[kGsChunk].x += wd.x * wd.x + wd.y * wd.y;
+            }
+        }
+        __syncthreads();
+    }
+    block_sum_v<kGsChunk + 1>(acc, sm);
+    if (threadIdx.x == 0) {
+        const double bad = __longlong_as_double(0x7ff8000000000000ll);
+#pragma unroll
+        for (int q = 0; q <= kGsChunk; ++q)
+            if (stalled) acc[q] = make_double2(bad, bad);
 #pragma unroll
         for (int q = 0; q < kGsChunk; ++q)
             if (q < nb) part[((size_t)k * no + i0 + q) * gridDim.x + blockIdx.x] = acc[q];
@@ -399,13 +545,15 @@ template <typename C> size_t GmresWork<C>::bytes() const {
     const size_t vec = sizeof(C) * (size_t)n * nrhs;
     return vec * (2 * (restart + 1) + 3) +
            sizeof(double2) * ((size_t)kGsBlocks * nrhs * (restart + 1) + 3 * (size_t)nrhs * (restart + 1) +
-                              (size_t)nrhs * (restart + 1) * (deflate + 1)) +
+                              (size_t)nrhs * (restart + 1) * (deflate + 1 + kMaxAug)) +
            sizeof(double) * 2 * nrhs;
 }
 
 template <typename C> tdda_status GmresWork<C>::init(long long n3, int nrhs_, int restart_, int degree_, int deflate_) {
     release();
     n = n3; nrhs = nrhs_; restart = restart_; degree = degree_; deflate = deflate_;
+    // the opt-in dynamic shared memory limit is a per-function attribute
+    TDDA_CUDA_TRY(cudaFuncSetAttribute(k_multidot_bulk<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBdSmem));
     const size_t vec = (size_t)n * nrhs;
     C **bufs[] = {&W, &Y, &U};
     for (C **b : bufs) TDDA_CUDA_TRY(cudaMalloc(b, sizeof(C) * vec));
@@ -418,7 +566,7 @@ template <typename C> tdda_status GmresWork<C>::init(long long n3, int nrhs_, in
     TDDA_CUDA_TRY(cudaMalloc(&part, sizeof(double2) * (size_t)kGsBlocks * nrhs * (restart + 1)));
     TDDA_CUDA_TRY(cudaMalloc(&h, sizeof(double2) * 2 * (size_t)nrhs * (restart + 1)));
     TDDA_CUDA_TRY(cudaMalloc(&coef, sizeof(double2) * (size_t)nrhs * (restart + 1)));
-    TDDA_CUDA_TRY(cudaMalloc(&P, sizeof(double2) * (size_t)nrhs * (restart + 1) * (deflate + 1)));
+    TDDA_CUDA_TRY(cudaMalloc(&P, sizeof(double2) * (size_t)nrhs * (restart + 1) * (deflate + 1 + kMaxAug)));
     TDDA_CUDA_TRY(cudaMalloc(&nrm, sizeof(double) * 2 * nrhs));
     TDDA_CUDA_TRY(cudaMallocHost(&h_host, sizeof(double2) * (2 * (size_t)nrhs * (restart + 1) + nrhs)));
     TDDA_CUDA_TRY(cudaMallocHost(&c_host, sizeof(double2) * (size_t)nrhs * (restart + 1)));
@@ -596,10 +744,12 @@ template <typename C> void multidot(GmresWork<C> &gw, int nv, const C *w, double
     unsigned nb;
     count_launches(2);
     if (packed(gw, w)) {
+        // two CTAs per SM over all chunks and right-hand sides
         const long long np = gw.n / E;
+        const long long ntiles = (np + kBdTile - 1) / kBdTile;
         nb = (unsigned)std::max<long long>(
-            1, std::min<long long>((np + kGsThreads * kMdPacks - 1) / (kGsThreads * kMdPacks), kGsBlocks));
-        launch_dep(k_multidot<C>, dim3(nb, nch, gw.nrhs), dim3(kGsThreads), 0, s, np, nv, nv + 1,
+            1, std::min<long long>({(2LL * 148) / ((long long)nch * gw.nrhs), ntiles, (long long)kGsBlocks}));
+        launch_dep(k_multidot_bulk<C>, dim3(nb, nch, gw.nrhs), dim3(kGsThreads), kBdSmem, s, np, nv, nv + 1,
                    (const PT *)gw.V, vstr / E, rstr / E, (const PT *)w, gw.part);
     } else {
         nb = gs_blocks(gw.n);
@@ -651,18 +801,15 @@ template <typename C> void scale_vec(GmresWork<C> &gw, const double *f, const C 
                out);
 }
 
-// One Arnoldi step on operator `op_fn` (v_j -> V[j+1]) with classical
+// Orthonormalises w (basis slot nv) against V[0..nv) with classical
 // Gram-Schmidt: one pass for the projections and the norm of w, one pass for
 // the update and the normalisation (the new norm by Pythagoras); when the
-// update cancels more than half of w the step takes a second projection pass
-// ("twice is enough").  The Hessenberg column of every right-hand side lands
-// in Hcol[k][0..j+1].
-template <typename C, class OpFn>
-tdda_status arnoldi_step(GmresWork<C> &gw, int j, OpFn op_fn, std::vector<std::vector<cplx>> &Hcol, cudaStream_t s) {
-    const int nv = j + 1, nr = gw.nrhs;
-    C *w = basis(gw, j + 1);
-    tdda_status st = op_fn(basis(gw, j), w);
-    if (st != TDDA_OK) return st;
+// update cancels more than half of w a second projection pass runs ("twice is
+// enough").  The coefficients of every right-hand side land in
+// Hcol[k][0..nv) and the remaining norm in Hcol[k][nv].
+template <typename C>
+tdda_status orthonormalise(GmresWork<C> &gw, int nv, C *w, std::vector<std::vector<cplx>> &Hcol, cudaStream_t s) {
+    const int nr = gw.nrhs;
     double2 *hh = gw.h_host;
     double2 *coef = gw.c_host;
     for (int k = 0; k < nr; ++k) Hcol[k].assign(nv + 1, cplx(0.0));
@@ -683,6 +830,11 @@ tdda_status arnoldi_step(GmresWork<C> &gw, int j, OpFn op_fn, std::vector<std::v
                 coef[(size_t)k * (nv + 1) + i] = hk[i];
             }
             const double wn2 = hk[nv].x;
+            if (!std::isfinite(wn2) || !std::isfinite(proj)) {
+                set_error("GMRES: non-finite Gram-Schmidt sums (a non-finite operator result, or a device wait "
+                          "in the projection kernel that gave up)");
+                return TDDA_ERR_BREAKDOWN;
+            }
             wp2[k] = wn2 - proj;
             if (wn2 > 0.0 && wp2[k] < 0.25 * wn2) cancel = true;
         }
@@ -696,6 +848,21 @@ tdda_status arnoldi_step(GmresWork<C> &gw, int j, OpFn op_fn, std::vector<std::v
         gs_update_scale(gw, nv, (const double2 *)gw.coef, w, s);
     }
     return TDDA_OK;
+}
+
+// One Arnoldi step on operator `op_fn`: w = op(V[j]) lands in V[j + 1 + aug]
+// and is orthonormalised against V[0..j + 1 + aug).  aug = 1 in the first
+// cycle of an inner solve that starts from a recycled space: there the new
+// right-hand side's direction sits in slot kd + 1, one ahead of the Arnoldi
+// sequence, so every column has two entries below its diagonal.  The column
+// of every right-hand side lands in Hcol[k][0..j + 1 + aug].
+template <typename C, class OpFn>
+tdda_status arnoldi_step(GmresWork<C> &gw, int j, OpFn op_fn, std::vector<std::vector<cplx>> &Hcol, cudaStream_t s,
+                         int aug = 0) {
+    C *w = basis(gw, j + 1 + aug);
+    tdda_status st = op_fn(basis(gw, j), w);
+    if (st != TDDA_OK) return st;
+    return orthonormalise(gw, j + 1 + aug, w, Hcol, s);
 }
 
 // Least-squares state of one right-hand side: the projected matrix Hbar
@@ -762,36 +929,50 @@ struct LsqState {
     }
 };
 
-// The deflated restart of GMRES-DR: from Hbar (k columns used, k = m), the
-// least-squares solution y and the start coefficients c0, the (m+1) x (kd+1)
-// orthonormal combination P (column-major, ld m+1) whose first kd columns
-// span the kd harmonic Ritz vectors of smallest magnitude and whose last
-// column is the residual's direction, the new projected matrix
-// P^H Hbar P[:m, :kd] ((kd+1) x kd) and the new start coefficients P^H rho.
-// Returns the number of deflation vectors kept (<= kd; 0 when the
-// eigenproblem failed: a plain restart).
+// The deflated restart of GMRES-DR: from Hbar (jc columns used, rows jc + 1,
+// or jc + 2 after a cycle that started from a recycled space; the rest of the
+// (m+1) x m storage is zero), the least-squares solution y and the start
+// coefficients c0, the orthonormal combination P ((m+1) x nc, column-major,
+// ld m+1) whose first kept columns span the kept harmonic Ritz vectors of
+// smallest magnitude and whose other rows - jc columns span the complement of
+// range(Hbar), the residual's direction first; the new projected matrix
+// P^H Hbar P[:m, :kept] (nc x kept) and the new start coefficients P^H rho.
+// Returns kept (<= kd); with kept = 0 (no vector asked for, or the
+// eigenproblem failed) P is the residual's direction alone: a plain restart.
 int deflated_restart(LsqState &L, int kd, const std::vector<cplx> &y, std::vector<cplx> &P,
-                     std::vector<cplx> &Hn, std::vector<cplx> &cn) {
+                     std::vector<cplx> &Hn, std::vector<cplx> &cn, int jc, int rows) {
     const int m = L.m, ld = m + 1;
     // residual coefficients rho = c0 - Hbar y
     std::vector<cplx> rho(L.c0);
     for (int j = 0; j < m; ++j)
         for (int i = 0; i <= m; ++i) rho[i] -= L.h(i, j) * y[j];
     std::vector<std::vector<cplx>> cols;
-    if (kd > 0) {
-        // harmonic Ritz pairs: (H_m + |h_{m+1,m}|^2 f e_m^T) g = theta g, H_m^H f = e_m
-        DenseMat Ht(m), M(m);
-        for (int i = 0; i < m; ++i)
-            for (int j = 0; j < m; ++j) {
+    if (kd > 0 && jc > 0) {
+        // harmonic Ritz pairs of span(V_jc): Hbar^H Hbar g = theta T^H g with
+        // T the top jc x jc block and B the rows below it, i.e.
+        // (T + T^-H B^H B) g = theta g  (B = h e_jc^T after a plain Arnoldi
+        // cycle: the usual rank-one update of the last column)
+        DenseMat Ht(jc), M(jc);
+        for (int i = 0; i < jc; ++i)
+            for (int j = 0; j < jc; ++j) {
                 Ht(i, j) = std::conj(L.h(j, i));
                 M(i, j) = L.h(i, j);
             }
-        std::vector<cplx> f(m, cplx(0.0));
-        f[m - 1] = 1.0;
-        bool ok = dense_solve(Ht.a.data(), m, m, f.data());
+        bool ok = true;
+        for (int b = jc; b < rows && ok; ++b) {
+            // f = T^-H conj(B row b); M += f B row b
+            std::vector<cplx> f(jc);
+            for (int i = 0; i < jc; ++i) f[i] = std::conj(L.h(b, i));
+            DenseMat Hw = Ht;
+            ok = dense_solve(Hw.a.data(), jc, jc, f.data());
+            if (ok)
+                for (int j = 0; j < jc; ++j) {
+                    const cplx bj = L.h(b, j);
+                    if (bj == cplx(0.0)) continue;
+                    for (int i = 0; i < jc; ++i) M(i, j) += f[i] * bj;
+                }
+        }
         if (ok) {
-            const double h2 = std::norm(L.h(m, m - 1));
-            for (int i = 0; i < m; ++i) M(i, m - 1) += h2 * f[i];
             std::vector<cplx> ev;
             ok = eigenpairs_few(M, ev, cols, [&](const std::vector<cplx> &e) {
                 std::vector<int> id(e.size());
@@ -826,12 +1007,13 @@ int deflated_restart(LsqState &L, int kd, const std::vector<cplx> &y, std::vecto
     };
     for (auto &c : cols) {
         std::vector<cplx> v(m + 1, cplx(0.0));
-        for (int i = 0; i < m; ++i) v[i] = c[i];
+        for (int i = 0; i < jc; ++i) v[i] = c[i];
         orth(v);
     }
     const int kept = (int)Q.size();
-    if (!orth(rho)) {
-        // the residual lies in the deflation space: keep its plain direction
+    if (!orth(rho) || kept == 0) {
+        // no deflation vector, or the residual lies in the deflation space:
+        // a plain restart from the residual's direction
         Q.clear();
         Q.push_back(rho);
         double nr = 0.0;
@@ -844,11 +1026,67 @@ int deflated_restart(LsqState &L, int kd, const std::vector<cplx> &y, std::vecto
         cn.assign(1, cplx(nr, 0.0));
         return 0;
     }
-    const int nc = kept + 1;
+    // Hbar g - theta [g; 0] lies in the complement of range(Hbar), which has
+    // rows - jc dimensions; the residual spans it after a plain Arnoldi cycle.
+    // Otherwise the rest of the complement joins the new basis, so that
+    // Ah V P[:, :kept] stays inside span(V P).
+    const int ext = rows - jc;
+    if (ext > 1) {
+        std::vector<std::vector<cplx>> Rg;  // orthonormal basis of range(Hbar)
+        for (int j = 0; j < jc; ++j) {
+            std::vector<cplx> v(m + 1, cplx(0.0));
+            for (int i = 0; i < rows; ++i) v[i] = L.h(i, j);
+            for (int pass = 0; pass < 2; ++pass)
+                for (auto &q : Rg) {
+                    cplx d = 0.0;
+                    for (int i = 0; i <= m; ++i) d += std::conj(q[i]) * v[i];
+                    for (int i = 0; i <= m; ++i) v[i] -= d * q[i];
+                }
+            double nv = 0.0;
+            for (auto &e : v) nv += std::norm(e);
+            nv = std::sqrt(nv);
+            if (!(nv > 0.0)) continue;
+            for (auto &e : v) e /= nv;
+            Rg.push_back(v);
+        }
+        // the unit vector whose complement part, with what P holds removed,
+        // is largest, until the complement is covered
+        for (int add = 1; add < ext; ++add) {
+            std::vector<cplx> best;
+            double bn = 0.0;
+            for (int a = 0; a < rows; ++a) {
+                std::vector<cplx> v(m + 1, cplx(0.0));
+                v[a] = 1.0;
+                for (int pass = 0; pass < 2; ++pass) {
+                    for (auto &q : Rg) {
+                        cplx d = std::conj(q[a]);
+                        if (pass == 1) {
+                            d = 0.0;
+                            for (int i = 0; i <= m; ++i) d += std::conj(q[i]) * v[i];
+                        }
+                        for (int i = 0; i <= m; ++i) v[i] -= d * q[i];
+                    }
+                    for (auto &q : Q) {
+                        cplx d = 0.0;
+                        for (int i = 0; i <= m; ++i) d += std::conj(q[i]) * v[i];
+                        for (int i = 0; i <= m; ++i) v[i] -= d * q[i];
+                    }
+                }
+                double nv = 0.0;
+                for (auto &e : v) nv += std::norm(e);
+                if (nv > bn) { bn = nv; best = v; }
+            }
+            if (!(bn > 1e-12) || !orth(best)) {
+                // the complement is not resolved: a plain restart
+                return deflated_restart(L, 0, y, P, Hn, cn, jc, rows);
+            }
+        }
+    }
+    const int nc = (int)Q.size();
     P.assign((size_t)ld * nc, cplx(0.0));
     for (int c = 0; c < nc; ++c)
         for (int i = 0; i <= m; ++i) P[i + (size_t)c * ld] = Q[c][i];
-    // Hn = P^H Hbar P[:m, :kept]  ((kept+1) x kept)
+    // Hn = P^H Hbar P[:m, :kept]  (nc x kept)
     std::vector<cplx> HP((size_t)ld * kept, cplx(0.0));
     for (int c = 0; c < kept; ++c)
         for (int j = 0; j < m; ++j) {
@@ -895,6 +1133,10 @@ tdda_status pgmres_solve(const RefineWork<C> &w, GmresWork<C> &gw, const double2
     std::vector<cplx> roots;
     std::vector<std::vector<cplx>> Hcol(nrhs);
     std::vector<LsqState> L(nrhs);
+    // the space carried from one inner solve to the next (o.recycle): slots
+    // 0..kr + ar of V, with Ah V[:, :kr] = V[:, :kr + ar + 1] Hr[k]
+    int kr = 0, ar = 0;
+    std::vector<std::vector<cplx>> Hr(nrhs);
     double *h = w.h_part;
     // the inner operator, and the inner operator times the polynomial
     auto op_plain = [&](const C *x, C *y) { return apply_scaled<C>(*w.op, w.sc, w.al, x, y, nrhs, w.dstride, s); };
@@ -953,14 +1195,32 @@ tdda_status pgmres_solve(const RefineWork<C> &w, GmresWork<C> &gw, const double2
         }
         TDDA_CUDA_TRY(cudaMemcpyAsync(w.d_part, h, sizeof(double) * 3 * nrhs, cudaMemcpyHostToDevice, s));
         launch_to_inner<C>(n, w.nbox, nrhs, w.dstride, w.Rm, w.d_part, w.sc64, w.R, s);
-        // V[0] = R^ / ||R^||, U = 0
-        gs_update(gw, 0, gw.h, 0, w.R, true, s);  // norms only
-        scale_vec(gw, gw.nrm + nrhs, w.R, basis(gw, 0), s);
-        TDDA_CUDA_TRY(cudaMemsetAsync(gw.U, 0, sizeof(C) * vstr, s));
-        TDDA_CUDA_TRY(cudaMemcpyAsync(gw.h_host, gw.nrm, sizeof(double) * nrhs, cudaMemcpyDeviceToHost, s));
-        TDDA_CUDA_TRY(cudaStreamSynchronize(s));
         std::vector<double> beta(nrhs);
-        for (int k = 0; k < nrhs; ++k) beta[k] = reinterpret_cast<const double *>(gw.h_host)[k];
+        // structure of the first cycle: aug extra directions below the
+        // Arnoldi sequence (0: plain GMRES(-DR) from R^)
+        int aug = 0;
+        if (kr > 0) {
+            // start from the recycled space: slots 0..kr + ar hold V_s with
+            // Ah V_s[:, :kr] = V_s Hr; R^ joins as slot kr + ar + 1
+            aug = ar + 1;
+            C *w0 = basis(gw, kr + aug);
+            TDDA_CUDA_TRY(cudaMemcpyAsync(w0, w.R, sizeof(C) * vstr, cudaMemcpyDeviceToDevice, s));
+            st = orthonormalise(gw, kr + aug, w0, Hcol, s);
+            if (st != TDDA_OK) return st;
+            for (int k = 0; k < nrhs; ++k) {
+                double b2 = 0.0;
+                for (const cplx &c : Hcol[k]) b2 += std::norm(c);
+                beta[k] = std::sqrt(b2);
+            }
+        } else {
+            // V[0] = R^ / ||R^||
+            gs_update(gw, 0, gw.h, 0, w.R, true, s);  // norms only
+            scale_vec(gw, gw.nrm + nrhs, w.R, basis(gw, 0), s);
+            TDDA_CUDA_TRY(cudaMemcpyAsync(gw.h_host, gw.nrm, sizeof(double) * nrhs, cudaMemcpyDeviceToHost, s));
+            TDDA_CUDA_TRY(cudaStreamSynchronize(s));
+            for (int k = 0; k < nrhs; ++k) beta[k] = reinterpret_cast<const double *>(gw.h_host)[k];
+        }
+        TDDA_CUDA_TRY(cudaMemsetAsync(gw.U, 0, sizeof(C) * vstr, s));
         if (roots.empty()) {
             // the polynomial: Arnoldi steps of the inner operator on the first
             // residual of the first unfinished right-hand side
@@ -993,13 +1253,22 @@ tdda_status pgmres_solve(const RefineWork<C> &w, GmresWork<C> &gw, const double2
             // V[0] is unchanged by those steps; the cycles overwrite V[1..]
         }
         // the inner solve: (deflated) restarted GMRES cycles on Ah p(Ah)
+        int kd = 0;                      // deflation vectors at the start of this cycle
         for (int k = 0; k < nrhs; ++k) {
             L[k].reset(m);
-            L[k].start({cplx(beta[k], 0.0)});
+            if (kr > 0) {
+                const int nc = kr + aug;   // rows of Hr: the recycled slots
+                for (int c = 0; c < kr; ++c)
+                    for (int r = 0; r < nc; ++r) L[k].h(r, c) = Hr[k][r + (size_t)c * nc];
+                L[k].start(Hcol[k]);
+            } else {
+                L[k].start({cplx(beta[k], 0.0)});
+            }
         }
-        int kd = 0;                      // deflation vectors at the start of this cycle
+        if (kr > 0) kd = kr;
+        kr = 0;                          // the recycled space is used up
         std::vector<double> cyc_prev(beta);
-        std::vector<int> inner_slow(nrhs, 0), inner_done(nrhs, 0);
+        std::vector<int> inner_slow(nrhs, 0), inner_done(nrhs, 0), last_cycle(nrhs, -1);
         for (int k = 0; k < nrhs; ++k) inner_done[k] = done[k];
         for (int cycle = 0;; ++cycle) {
             int jc = kd;                 // columns of Hbar filled
@@ -1007,14 +1276,14 @@ tdda_status pgmres_solve(const RefineWork<C> &w, GmresWork<C> &gw, const double2
                 if (!inner_done[k])
                     for (int j = 0; j < kd; ++j) L[k].add(j);
             bool reached = false;
-            for (int j = kd; j < m; ++j) {
-                st = arnoldi_step(gw, j, op_poly, Hcol, s);
+            for (int j = kd; j < m - aug; ++j) {
+                st = arnoldi_step(gw, j, op_poly, Hcol, s, aug);
                 if (st != TDDA_OK) return st;
                 jc = j + 1;
                 reached = true;
                 for (int k = 0; k < nrhs; ++k) {
                     if (inner_done[k]) continue;
-                    for (int i = 0; i <= j + 1; ++i) L[k].h(i, j) = Hcol[k][i];
+                    for (int i = 0; i <= j + 1 + aug; ++i) L[k].h(i, j) = Hcol[k][i];
                     const double est = L[k].add(j);
                     mv[k] += (long long)roots.size();
                     steps[k] += 1;
@@ -1022,6 +1291,7 @@ tdda_status pgmres_solve(const RefineWork<C> &w, GmresWork<C> &gw, const double2
                 }
                 if (reached) break;
             }
+            const int rows = jc + 1 + aug;
             // u += V y over the jc columns
             std::vector<double2> coef((size_t)nrhs * jc, make_double2(0.0, 0.0));
             std::vector<std::vector<cplx>> ys(nrhs);
@@ -1037,7 +1307,10 @@ tdda_status pgmres_solve(const RefineWork<C> &w, GmresWork<C> &gw, const double2
                 // solve has given what it can; the refinement takes over
                 inner_slow[k] = (est > 0.995 * cyc_prev[k]) ? inner_slow[k] + 1 : 0;
                 cyc_prev[k] = est;
-                if (est <= h[2 * nrhs + k] * beta[k] || mv[k] >= max_iter || inner_slow[k] >= 12) inner_done[k] = 1;
+                if (est <= h[2 * nrhs + k] * beta[k] || mv[k] >= max_iter || inner_slow[k] >= 12) {
+                    inner_done[k] = 1;
+                    last_cycle[k] = cycle;
+                }
                 all_in &= (inner_done[k] != 0);
             }
             TDDA_CUDA_TRY(cudaMemcpyAsync(gw.coef, coef.data(), sizeof(double2) * coef.size(), cudaMemcpyHostToDevice, s));
@@ -1047,38 +1320,47 @@ tdda_status pgmres_solve(const RefineWork<C> &w, GmresWork<C> &gw, const double2
             // U += W (the combination lands in W first: k_lincomb overwrites)
             count_launches(1);
             launch_dep(k_axpy_c<C>, dim3(gs_blocks(n * nrhs)), dim3(kGsThreads), 0, s, n * nrhs, (const C *)gw.W, gw.U);
-            if (all_in || cycle > 100000) break;
-            // restart: deflated (GMRES-DR) or plain from the current residual
+            // the deflated restart, or (recycling, once the inner solve ends
+            // with every right-hand side of this step finishing in this cycle)
+            // the space the next refinement step starts from
+            bool save = false;
+            if (all_in) {
+                // (room for the carried space plus two Arnoldi steps per cycle)
+                save = o.recycle && o.deflate > 0 && aug < kMaxAug && o.deflate + kMaxAug + 2 <= m;
+                for (int k = 0; k < nrhs; ++k)
+                    if (!done[k] && last_cycle[k] != cycle) save = false;
+                if (!save) break;
+            } else if (cycle > 100000) {
+                break;
+            }
             std::vector<std::vector<cplx>> Ps(nrhs), Hns(nrhs), cns(nrhs);
-            int kept = o.deflate;
-            for (int k = 0; k < nrhs; ++k) {
-                if (inner_done[k]) continue;
+            auto restart_k = [&](int k, int want) {
                 std::vector<cplx> yfull(m, cplx(0.0));
                 for (int i = 0; i < jc; ++i) yfull[i] = ys[k][i];
-                kept = std::min(kept, deflated_restart(L[k], o.deflate, yfull, Ps[k], Hns[k], cns[k]));
-            }
+                return deflated_restart(L[k], want, yfull, Ps[k], Hns[k], cns[k], jc, rows);
+            };
+            auto active = [&](int k) { return save ? !done[k] : !inner_done[k]; };
+            int kept = o.deflate;
+            for (int k = 0; k < nrhs; ++k)
+                if (active(k)) kept = std::min(kept, restart_k(k, o.deflate));
             // every right-hand side keeps the same number of vectors
             for (int k = 0; k < nrhs; ++k) {
-                if (inner_done[k]) continue;
-                const int have = (int)(Ps[k].size() / ld) - 1;
+                if (!active(k)) continue;
+                const int have = Hns[k].empty() ? 0 : (int)(Hns[k].size() / (Ps[k].size() / ld));
                 if (have != kept) {
-                    std::vector<cplx> yfull(m, cplx(0.0));
-                    for (int i = 0; i < jc; ++i) yfull[i] = ys[k][i];
-                    deflated_restart(L[k], kept, yfull, Ps[k], Hns[k], cns[k]);
-                    if ((int)(Ps[k].size() / ld) - 1 != kept) kept = 0;
+                    restart_k(k, kept);
+                    const int got = Hns[k].empty() ? 0 : (int)(Hns[k].size() / (Ps[k].size() / ld));
+                    if (got != kept) kept = 0;
                 }
             }
             if (kept == 0)
-                for (int k = 0; k < nrhs; ++k) {
-                    if (inner_done[k]) continue;
-                    std::vector<cplx> yfull(m, cplx(0.0));
-                    for (int i = 0; i < jc; ++i) yfull[i] = ys[k][i];
-                    deflated_restart(L[k], 0, yfull, Ps[k], Hns[k], cns[k]);
-                }
-            const int nc = kept + 1;
+                for (int k = 0; k < nrhs; ++k)
+                    if (active(k)) restart_k(k, 0);
+            if (save && kept == 0) break;   // nothing worth carrying over
+            const int nc = kept == 0 ? 1 : kept + rows - jc;
             std::vector<double2> Pd((size_t)nrhs * ld * nc, make_double2(0.0, 0.0));
             for (int k = 0; k < nrhs; ++k) {
-                if (inner_done[k]) continue;
+                if (!active(k)) continue;
                 for (int i = 0; i <= m; ++i)
                     for (int c = 0; c < nc; ++c) {
                         const cplx v = Ps[k][i + (size_t)c * ld];
@@ -1100,6 +1382,13 @@ tdda_status pgmres_solve(const RefineWork<C> &w, GmresWork<C> &gw, const double2
                 std::swap(gw.V, gw.V2);
             }
             TDDA_CUDA_TRY(cudaGetLastError());
+            if (save) {
+                // slots 0..nc-1: Ah V[:, :kept] = V Hr (nc x kept)
+                kr = kept;
+                ar = nc - kept - 1;
+                for (int k = 0; k < nrhs; ++k) Hr[k] = active(k) ? Hns[k] : std::vector<cplx>();
+                break;
+            }
             for (int k = 0; k < nrhs; ++k) {
                 if (inner_done[k]) continue;
                 L[k].reset(m);
@@ -1108,6 +1397,7 @@ tdda_status pgmres_solve(const RefineWork<C> &w, GmresWork<C> &gw, const double2
                 L[k].start(cns[k]);
             }
             kd = kept;
+            aug = kept == 0 ? 0 : nc - kept - 1;
         }
         // correction D = p(Ah) U, X += ||R|| S D
         for (int i = 0; i < (int)roots.size(); ++i) {

@@ -38,7 +38,7 @@ template <typename C> struct GmresWork {
     double2 *h = nullptr;       // device sums [2][nrhs][restart + 1]
     double *nrm = nullptr;      // device norms / reciprocals [2][nrhs]
     double2 *coef = nullptr;    // device [nrhs][restart + 1] combination weights
-    double2 *P = nullptr;       // device [nrhs][restart + 1][deflate + 1] restart combinations
+    double2 *P = nullptr;       // device [nrhs][restart + 1][deflate + 1 + 4] restart combinations
     double2 *h_host = nullptr;  // pinned mirror of h, nrm
     double2 *c_host = nullptr;  // pinned staging of coef
     tdda_status init(long long n3, int nrhs, int restart, int degree, int deflate);
@@ -52,6 +52,10 @@ struct GmresOptions {
     int restart = 40;       // GMRES steps per cycle
     int deflate = 0;        // harmonic Ritz vectors kept across restarts (GMRES-DR), < restart
     double floor = 0.0;     // an inner solve stops once it has cut its residual by this much
+    // carry the deflation space from one refinement step's inner solve to the
+    // next (needs deflate > 0): the next inner solve starts from that space
+    // with the new residual added to it, instead of from the residual alone
+    bool recycle = false;
 };
 
 // Solves (A + diag al) X = B to a TRUE relative residual <= tol per

@@ -1435,16 +1435,21 @@ tdda_status tdda_filter_state(tdda_model *m, double *raw, double *filtered, int6
 
 tdda_status tdda_set_solver(tdda_model *m, int kind, int degree, int restart, int deflate) {
     if (m == nullptr) return bad("null model");
-    if (kind != 0 && kind != 1) return bad("solver must be 0 (BiCGSTAB) or 1 (polynomial-preconditioned GMRES)");
-    if (kind == 1) {
+    if (kind < 0 || kind > 2)
+        return bad("solver must be 0 (BiCGSTAB), 1 (polynomial-preconditioned GMRES) or 2 (GMRES carrying its "
+                   "deflation space across refinement steps)");
+    if (kind >= 1) {
         if (degree < 1 || degree > 64) return bad("polynomial degree must be in [1, 64]");
         if (restart < 2 || restart > 1024) return bad("GMRES restart must be in [2, 1024]");
         if (deflate < 0 || deflate >= restart) return bad("deflation vectors must be in [0, restart)");
+        if (kind == 2 && (deflate < 1 || deflate + 6 > restart))
+            return bad("carrying the deflation space needs 1 <= deflate <= restart - 6");
         m->gopt.degree = degree;
         m->gopt.restart = restart;
         m->gopt.deflate = deflate;
+        m->gopt.recycle = kind == 2;
     }
-    m->solver = kind;
+    m->solver = kind == 0 ? 0 : 1;
     return TDDA_OK;
 }
 

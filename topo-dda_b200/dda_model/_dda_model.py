@@ -327,8 +327,10 @@ class DDAModel:
         Jacobi-scaled operator times a polynomial of `degree` in it, cycles of
         `restart` steps keeping `deflate` harmonic Ritz vectors across restarts,
         inside complex128 refinement (for structures that fill their periodic
-        cell, where BiCGSTAB stalls)."""
-        k = {"bicgstab": 0, "pgmres": 1}[kind]
+        cell, where BiCGSTAB stalls).  "gmres-dr-recycle": "pgmres" whose inner
+        solve of each refinement step after the first starts from the deflation
+        space the previous inner solve ended with."""
+        k = {"bicgstab": 0, "pgmres": 1, "gmres-dr-recycle": 2}[kind]
         _lib.check(self._lib.tdda_set_solver(self._handle, k, int(degree), int(restart), int(deflate)))
 
     @staticmethod

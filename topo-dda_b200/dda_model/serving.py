@@ -196,6 +196,7 @@ def synthetic_stream(n=512, rate=200.0, seed=7, shapes=SERVE_SHAPES, lam_range=(
 @dataclass
 class StreamReport:
     results: list = field(default_factory=list)
+    requests: list = field(default_factory=list)
     wall_s: float = 0.0
     latency_ms: np.ndarray = None
 
@@ -211,6 +212,26 @@ class StreamReport:
             "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
             "mean_ms": float(lat.mean()), "max_true_error": max(i["true_error"] for r in self.results for i in r.info),
         }
+
+    def per_shape(self):
+        """Per grid: requests, mean batch size (right-hand sides), batches,
+        device-side solve time of a batch (median), the GPU seconds the grid's
+        batches took in total (each batch counted once), and the mean inner
+        iterations per right-hand side."""
+        out = {}
+        shapes = [tuple(q.shape) for q in self.requests]
+        for shape in sorted(set(shapes)):
+            rs = [r for r, sh in zip(self.results, shapes) if sh == shape]
+            key = "x".join(str(v) for v in shape)
+            out[key] = {
+                "requests": len(rs),
+                "batches": sum(1.0 / r.batch_requests for r in rs),
+                "mean_batch_rhs": float(np.mean([r.batch_rhs for r in rs])),
+                "median_batch_solve_ms": float(np.median([r.solve_ms for r in rs])),
+                "solve_s_total": sum(r.solve_ms / r.batch_requests for r in rs) / 1e3,
+                "mean_inner_iterations": float(np.mean([i["inner_iterations"] for r in rs for i in r.info])),
+            }
+        return out
 
 
 def run_stream(server: DDAServer, requests, realtime=True) -> StreamReport:
@@ -246,6 +267,6 @@ def run_stream(server: DDAServer, requests, realtime=True) -> StreamReport:
     th.join()
     if errors:
         raise errors[0]
-    rep = StreamReport(results=results, wall_s=time.perf_counter() - t0)
+    rep = StreamReport(results=results, requests=list(requests), wall_s=time.perf_counter() - t0)
     rep.latency_ms = np.array([r.total_ms for r in results])
     return rep
