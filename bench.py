@@ -61,7 +61,7 @@ for _p in (ROOT, os.path.join(ROOT, "topo-dda_b200")):
 MAX_ITER = 400000  # inner operator applications per solve; the benchmark solves converge well below this
 # solver of the periodic workloads: GMRES on the scaled operator times a polynomial of
 # `degree`, cycles of `restart` steps keeping `deflate` harmonic Ritz vectors
-SOLVER = dict(degree=1, restart=60, deflate=20)
+SOLVER = dict(degree=1, restart=40, deflate=10)
 _T0 = time.perf_counter()
 
 

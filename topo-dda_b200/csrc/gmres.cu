@@ -71,63 +71,7 @@ template <> struct Pack<double2> {
 
 // part[(k * no + i) * gridDim.x + blk] = this block's share of conj(V_i[k]) . w[k]
 // for i < nv; with no = nv + 1 the CTAs of the first chunk also sum ||w[k]||^2
-// into entry i = nv.  Lengths and strides in packs.  A thread takes kMdPacks
-// packs per round and issues the loads of all of them (kGsChunk basis vectors
-// each, 16 x 16 bytes) before using any: on B200 at 1.57 M complex64 elements
-// this streams 5.1 TB/s against 4.5 TB/s for one element per thread.
-constexpr int kMdPacks = 2;
-
-template <typename C>
-__global__ void __launch_bounds__(kGsThreads) k_multidot(long long np, int nv, int no,
-                                                         const typename Pack<C>::T *__restrict__ V, size_t vstr,
-                                                         size_t rstr, const typename Pack<C>::T *__restrict__ w,
-                                                         double2 *__restrict__ part) {
-    using PK = Pack<C>;
-    using PT = typename PK::T;
-    pdl_wait();
-    __shared__ double2 sm[(kGsChunk + 1) * (kGsThreads / 32)];
-    const int k = blockIdx.z, i0 = blockIdx.y * kGsChunk;
-    const int nb = min(kGsChunk, nv - i0);
-    const bool norm = no > nv && blockIdx.y == 0;
-    double2 acc[kGsChunk + 1];
-#pragma unroll
-    for (int q = 0; q <= kGsChunk; ++q) acc[q] = make_double2(0.0, 0.0);
-    const PT *wk = w + (size_t)k * rstr;
-    const PT *Vk = V + (size_t)k * rstr + (size_t)i0 * vstr;
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long p0 = (long long)blockIdx.x * blockDim.x + threadIdx.x; p0 < np; p0 += kMdPacks * stride) {
-        PT wv[kMdPacks], v[kMdPacks][kGsChunk];
-#pragma unroll
-        for (int u = 0; u < kMdPacks; ++u) {
-            const long long p = p0 + u * stride;
-            const bool in = p < np;
-            wv[u] = in ? __ldg(wk + p) : PK::zero();
-#pragma unroll
-            for (int q = 0; q < kGsChunk; ++q) v[u][q] = (in && q < nb) ? __ldg(Vk + (size_t)q * vstr + p) : PK::zero();
-        }
-#pragma unroll
-        for (int u = 0; u < kMdPacks; ++u)
-#pragma unroll
-            for (int e = 0; e < PK::E; ++e) {
-                const double2 wd = PK::get(wv[u], e);
-#pragma unroll
-                for (int q = 0; q < kGsChunk; ++q) {
-                    const double2 d = cdot1(PK::get(v[u][q], e), wd);
-                    acc[q].x += d.x;
-                    acc[q].y += d.y;
-                }
-                if (norm) acc[kGsChunk].x += wd.x * wd.x + wd.y * wd.y;
-            }
-    }
-    block_sum_v<kGsChunk + 1>(acc, sm);
-    if (threadIdx.x == 0) {
-#pragma unroll
-        for (int q = 0; q < kGsChunk; ++q)
-            if (q < nb) part[((size_t)k * no + i0 + q) * gridDim.x + blockIdx.x] = acc[q];
-        if (norm) part[((size_t)k * no + nv) * gridDim.x + blockIdx.x] = acc[kGsChunk];
-    }
-}
-
+// into entry i = nv.
 // The same sums with the vectors streamed into shared memory by the bulk-copy
 // engine (cp.async.bulk, global -> shared, completion on an mbarrier): tiles
 // of kBdTile packs of w and of every basis vector of the CTA's chunk, kBdStages
@@ -476,29 +420,6 @@ __global__ void __launch_bounds__(kGsThreads) k_scale_vec(long long n, size_t rs
     }
 }
 
-// out[k] = sum_{i < nv} y[k * ystr + i] V_i[k]
-template <typename C>
-__global__ void __launch_bounds__(kGsThreads) k_lincomb(long long n, int nv, const C *__restrict__ V, size_t vstr,
-                                                        size_t rstr, const double2 *__restrict__ y, int ystr,
-                                                        C *__restrict__ out) {
-    pdl_wait();
-    extern __shared__ double2 ys[];
-    const int k = blockIdx.z;
-    for (int i = threadIdx.x; i < nv; i += blockDim.x) ys[i] = y[(size_t)k * ystr + i];
-    __syncthreads();
-    const C *Vk = V + (size_t)k * rstr;
-    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
-        double2 v = make_double2(0.0, 0.0);
-        for (int i = 0; i < nv; ++i) {
-            const double2 b = to_d(__ldg(Vk + (size_t)i * vstr + e));
-            const double2 c = ys[i];
-            v.x += c.x * b.x - c.y * b.y;
-            v.y += c.x * b.y + c.y * b.x;
-        }
-        out[(size_t)k * rstr + e] = from_d<C>(v);
-    }
-}
-
 // out_l[k] = sum_{i < nin} P[k][i * ldp + l] V_i[k] for l < nout (in chunks of
 // kGsChunk outputs per CTA row): the deflated restart's new basis
 template <typename C>
@@ -527,6 +448,78 @@ __global__ void __launch_bounds__(kGsThreads) k_lincomb_multi(long long n, int n
 #pragma unroll
         for (int q = 0; q < kGsChunk; ++q)
             if (q < nb) out[(size_t)(l0 + q) * vstr + (size_t)k * rstr + e] = from_d<C>(acc[q]);
+    }
+}
+
+// out_l[k] = sum_{i < nin} P[k * pstr + i * ldp + l] V_i[k] for l < nout, in
+// 16-byte packs: one pack per thread and NB outputs per CTA row, the
+// coefficients of the CTA's outputs in shared memory (read as broadcasts),
+// the loads of four inputs issued before their products.  Used by the
+// deflated restart (NB = 8) and the cycle correction (NB = 1); lengths and
+// strides in packs.
+template <typename C, int NB>
+__global__ void __launch_bounds__(kGsThreads) k_lincomb_pack(long long np, int nin, int nout,
+                                                             const typename Pack<C>::T *__restrict__ V, size_t vstr,
+                                                             size_t rstr, const double2 *__restrict__ P, int ldp,
+                                                             size_t pstr, typename Pack<C>::T *__restrict__ out) {
+    using PK = Pack<C>;
+    using PT = typename PK::T;
+    constexpr int E = PK::E;
+    pdl_wait();
+    extern __shared__ double2 cs[];   // [nin][NB]
+    const int k = blockIdx.z, l0 = blockIdx.y * NB;
+    const int nb = min(NB, nout - l0);
+    for (int t = threadIdx.x; t < nin * NB; t += blockDim.x) {
+        const int i = t / NB, q = t % NB;
+        cs[t] = q < nb ? P[(size_t)k * pstr + (size_t)i * ldp + l0 + q] : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    const PT *Vk = V + (size_t)k * rstr;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < np; p += (long long)gridDim.x * blockDim.x) {
+        double2 acc[E][NB];
+#pragma unroll
+        for (int e = 0; e < E; ++e)
+#pragma unroll
+            for (int q = 0; q < NB; ++q) acc[e][q] = make_double2(0.0, 0.0);
+        int i = 0;
+        for (; i + 4 <= nin; i += 4) {
+            PT b[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) b[u] = __ldg(Vk + (size_t)(i + u) * vstr + p);
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int e = 0; e < E; ++e) {
+                    const double2 bd = PK::get(b[u], e);
+#pragma unroll
+                    for (int q = 0; q < NB; ++q) {
+                        const double2 c = cs[(i + u) * NB + q];
+                        acc[e][q].x += c.x * bd.x - c.y * bd.y;
+                        acc[e][q].y += c.x * bd.y + c.y * bd.x;
+                    }
+                }
+        }
+        for (; i < nin; ++i) {
+            const PT b = __ldg(Vk + (size_t)i * vstr + p);
+#pragma unroll
+            for (int e = 0; e < E; ++e) {
+                const double2 bd = PK::get(b, e);
+#pragma unroll
+                for (int q = 0; q < NB; ++q) {
+                    const double2 c = cs[i * NB + q];
+                    acc[e][q].x += c.x * bd.x - c.y * bd.y;
+                    acc[e][q].y += c.x * bd.y + c.y * bd.x;
+                }
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < NB; ++q)
+            if (q < nb) {
+                double2 d[E];
+#pragma unroll
+                for (int e = 0; e < E; ++e) d[e] = acc[e][q];
+                out[(size_t)(l0 + q) * vstr + (size_t)k * rstr + p] = PK::make(d);
+            }
     }
 }
 
@@ -792,6 +785,33 @@ void gs_update(GmresWork<C> &gw, int nv, const double2 *h, int hstr, C *w, bool 
         count_launches(1);
         launch_dep(k_sum_parts, dim3((gw.nrhs + 7) / 8), dim3(256), 0, s, gw.nrhs, (int)nb, (const double2 *)gw.part,
                    (double2 *)nullptr, gw.nrm, gw.nrm + gw.nrhs);
+    }
+}
+
+// out_l[k] = sum_{i < nin} P[k * pstr + i * ldp + l] V_i[k], l < nout (device
+// coefficients; out has the basis layout: vector l of right-hand side k at
+// l * vstr + k * n)
+template <typename C>
+void lincomb(GmresWork<C> &gw, int nin, int nout, const C *V, const double2 *P, int ldp, size_t pstr, C *out,
+             cudaStream_t s) {
+    using PT = typename Pack<C>::T;
+    constexpr int E = Pack<C>::E;
+    const size_t vstr = (size_t)gw.n * gw.nrhs;
+    count_launches(1);
+    const bool pk = gw.n % E == 0 && ((uintptr_t)V & 15) == 0 && ((uintptr_t)out & 15) == 0;
+    if (pk && nout == 1 && (size_t)nin * sizeof(double2) <= 48 * 1024) {
+        const long long np = gw.n / E;
+        launch_dep(k_lincomb_pack<C, 1>, dim3(gs_blocks(np), 1, gw.nrhs), dim3(kGsThreads),
+                   sizeof(double2) * nin, s, np, nin, 1, (const PT *)V, vstr / E, (size_t)gw.n / E, P, ldp, pstr,
+                   (PT *)out);
+    } else if (pk && (size_t)nin * kGsChunk * sizeof(double2) <= 48 * 1024) {
+        const long long np = gw.n / E;
+        launch_dep(k_lincomb_pack<C, kGsChunk>, dim3(gs_blocks(np), (nout + kGsChunk - 1) / kGsChunk, gw.nrhs),
+                   dim3(kGsThreads), sizeof(double2) * nin * kGsChunk, s, np, nin, nout, (const PT *)V, vstr / E,
+                   (size_t)gw.n / E, P, ldp, pstr, (PT *)out);
+    } else {
+        launch_dep(k_lincomb_multi<C>, dim3(gs_blocks(gw.n), (nout + kGsChunk - 1) / kGsChunk, gw.nrhs),
+                   dim3(kGsThreads), 0, s, gw.n, nin, nout, V, vstr, (size_t)gw.n, P, ldp, pstr, out);
     }
 }
 
@@ -1314,9 +1334,7 @@ tdda_status pgmres_solve(const RefineWork<C> &w, GmresWork<C> &gw, const double2
                 all_in &= (inner_done[k] != 0);
             }
             TDDA_CUDA_TRY(cudaMemcpyAsync(gw.coef, coef.data(), sizeof(double2) * coef.size(), cudaMemcpyHostToDevice, s));
-            count_launches(1);
-            launch_dep(k_lincomb<C>, dim3(gs_blocks(n), 1, nrhs), dim3(kGsThreads), sizeof(double2) * jc, s, n, jc,
-                       (const C *)gw.V, vstr, (size_t)n, (const double2 *)gw.coef, jc, gw.W);
+            lincomb(gw, jc, 1, (const C *)gw.V, (const double2 *)gw.coef, 1, (size_t)jc, gw.W, s);
             // U += W (the combination lands in W first: k_lincomb overwrites)
             count_launches(1);
             launch_dep(k_axpy_c<C>, dim3(gs_blocks(n * nrhs)), dim3(kGsThreads), 0, s, n * nrhs, (const C *)gw.W, gw.U);
@@ -1370,15 +1388,10 @@ tdda_status pgmres_solve(const RefineWork<C> &w, GmresWork<C> &gw, const double2
             TDDA_CUDA_TRY(cudaMemcpyAsync(gw.P, Pd.data(), sizeof(double2) * Pd.size(), cudaMemcpyHostToDevice, s));
             if (nc == 1) {
                 // plain restart: V[0] = V P in place of a second basis
-                count_launches(1);
-                launch_dep(k_lincomb_multi<C>, dim3(gs_blocks(n), 1, nrhs), dim3(kGsThreads), 0, s, n, m + 1, 1,
-                           (const C *)gw.V, vstr, (size_t)n, (const double2 *)gw.P, 1, (size_t)ld, gw.W);
+                lincomb(gw, m + 1, 1, (const C *)gw.V, (const double2 *)gw.P, 1, (size_t)ld, gw.W, s);
                 TDDA_CUDA_TRY(cudaMemcpyAsync(gw.V, gw.W, sizeof(C) * vstr, cudaMemcpyDeviceToDevice, s));
             } else {
-                count_launches(1);
-                launch_dep(k_lincomb_multi<C>, dim3(gs_blocks(n), (nc + kGsChunk - 1) / kGsChunk, nrhs),
-                           dim3(kGsThreads), 0, s, n, m + 1, nc, (const C *)gw.V, vstr, (size_t)n,
-                           (const double2 *)gw.P, nc, (size_t)ld * nc, gw.V2);
+                lincomb(gw, m + 1, nc, (const C *)gw.V, (const double2 *)gw.P, nc, (size_t)ld * nc, gw.V2, s);
                 std::swap(gw.V, gw.V2);
             }
             TDDA_CUDA_TRY(cudaGetLastError());
