@@ -62,6 +62,9 @@ MAX_ITER = 400000  # inner operator applications per solve; the benchmark solves
 # solver of the periodic workloads: GMRES on the scaled operator times a polynomial of
 # `degree`, cycles of `restart` steps keeping `deflate` harmonic Ritz vectors
 SOLVER = dict(degree=1, restart=40, deflate=10)
+# basis vectors a Gram-Schmidt pass reads on average in a GMRES-DR(40, 10)
+# cycle (11 to 40 after a deflated restart)
+GS_NV = 25
 _T0 = time.perf_counter()
 
 
@@ -89,6 +92,9 @@ def parse():
     ap.add_argument("--profile-matvec", type=int, default=0, metavar="K",
                     help="only build the benchmark model and apply the operator K times per precision "
                          "(the case the kernel profiles capture); prints per-pass times")
+    ap.add_argument("--profile-gs", type=int, default=0, metavar="K",
+                    help="time K projection and K update passes of the Gram-Schmidt kernels against "
+                         "GS_NV complex64 basis vectors of the benchmark grid, then exit (profiling case)")
     ap.add_argument("--profile-gmres", type=int, default=0, metavar="K",
                     help="profile case of the GMRES-DR kernels: one mixed-precision solve of the x-polarised "
                          "RHS of the benchmark structure, capped at K inner operator applications; prints the "
@@ -230,10 +236,11 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def traffic_record():
-    """DRAM bytes per fused complex64 matvec from the committed ncu summary
-    (profiles/matvec_c64_traffic.txt: 'key: value' lines)."""
-    path = os.path.join(ROOT, "profiles", "matvec_c64_traffic.txt")
+def traffic_record(name="matvec_c64_traffic.txt"):
+    """DRAM bytes per launch from a committed ncu summary under profiles/
+    ('key: value' lines): the fused complex64 matvec, or the Gram-Schmidt
+    projection kernel."""
+    path = os.path.join(ROOT, "profiles", name)
     if not os.path.exists(path):
         return None
     rec = {}
@@ -770,6 +777,10 @@ def main():
     m = pair.models[0]
     log(f"models built in {setup_s:.2f} s (lattice {m.info['lattice_ms']:.1f} ms, tensor FFT "
         f"{m.info['tensor_fft_ms']:.1f} ms)")
+    if args.profile_gs > 0:
+        ms = m.profile_gram_schmidt("mixed", GS_NV, args.profile_gs)
+        print(json.dumps({"nv": GS_NV, "ms_projection": ms[0], "ms_update": ms[1]}))
+        return 0
     if args.profile_matvec > 0:
         for prec in ("mixed", "complex128"):
             ms, passes = m.profile_matvec(prec, nrhs=1, iters=args.profile_matvec)
@@ -819,6 +830,11 @@ def main():
     # roofline of the dominant kernel: the complex64 fused matvec (3 passes)
     ms64, pass64 = m.profile_matvec("mixed", nrhs=1, iters=20)
     ms128, pass128 = m.profile_matvec("complex128", nrhs=1, iters=10)
+    # the largest single kernel of the solve: the Gram-Schmidt projection pass
+    gs_proj, gs_upd = m.profile_gram_schmidt("mixed", GS_NV, 20)
+    gs_bytes = (GS_NV + 1) * 3.0 * N * 8
+    gs_upd_bytes = (GS_NV + 2) * 3.0 * N * 8
+    trg = traffic_record("k_multidot_bulk_gs_traffic.txt") or {}
     peak, peak_kind = peaks()
     b64 = 824.0 * N
     b128 = 1648.0 * N
@@ -917,13 +933,26 @@ def main():
                                steps=plain_steps),
             "mixed_over_plain": value / plain,
             "reference_algorithm_gpu": ref_alg,
+            "roofline_gram_schmidt": {"bound": "hbm", "achieved": gs_bytes / (gs_proj * 1e-3) / 1e9, "peak": peak,
+                         "unit": "GB/s", "frac": gs_bytes / (gs_proj * 1e-3) / 1e9 / peak, "peak_kind": peak_kind,
+                         "traffic": trg.get("bytes_per_launch"),
+                         "traffic_source": "profiles/k_multidot_bulk_gs_traffic.txt (ncu dram bytes, nv = 25)",
+                         "kernel": f"k_multidot_bulk<float2> (GMRES projections V^H w and ||w||^2 against "
+                                   f"{GS_NV} basis vectors, + block sums), 22% of the solve's device time "
+                                   f"(profiles/launches_gmres_solve_128x128x32.md)",
+                         "algorithmic_bytes": gs_bytes, "ms": gs_proj,
+                         "update": {"kernel": "k_gs_update_scale<float2>", "ms": gs_upd,
+                                    "achieved": gs_upd_bytes / (gs_upd * 1e-3) / 1e9,
+                                    "frac": gs_upd_bytes / (gs_upd * 1e-3) / 1e9 / peak}},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": (tr or {}).get("bytes_per_launch_cold"),
                          "traffic_warm": (tr or {}).get("bytes_per_launch_warm"),
                          "dram_frac": ((tr or {}).get("bytes_per_launch_cold") or 0) / (ms64 * 1e-3) / 1e9 / peak,
                          "traffic_source": "profiles/matvec_c64_traffic.txt (ncu dram bytes, 3 passes, 1 RHS)",
-                         "kernel": "fused complex64 matvec (3 passes), 1 RHS",
+                         "kernel": "fused complex64 matvec (3 passes), 1 RHS: 48% of the solve's device time, its "
+                                   "pass 2 (k_xconv_reg, 24%) the largest single kernel "
+                                   "(profiles/launches_gmres_solve_128x128x32.md)",
                          "algorithmic_bytes": b64, "ms": ms64, "pass_ms": pass64,
                          "c128": {"ms": ms128, "achieved": b128 / (ms128 * 1e-3) / 1e9,
                                   "frac": b128 / (ms128 * 1e-3) / 1e9 / peak, "pass_ms": pass128},

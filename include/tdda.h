@@ -224,6 +224,13 @@ tdda_status tdda_patch_gradient(tdda_model *m, int max_iter, double tol, double 
  * 1 complex64 (mixed-precision models only). */
 tdda_status tdda_profile_matvec(tdda_model *m, int precision, int nrhs, int iters, double *ms_matvec,
                                 double *ms_pass);
+/* Timing of the GMRES Gram-Schmidt kernels on the model's stream (CUDA events;
+ * no reference counterpart, measurement support): on a scratch basis of nv
+ * vectors of the model's size (3 * nx*ny*nz elements, complex128 for precision
+ * 0, complex64 for 1), ms[0] = mean time of one projection pass (V^H w and
+ * ||w||^2: the bulk-copy kernel and its block sums), ms[1] = mean time of one
+ * update and normalisation pass.  Allocates and frees the scratch basis. */
+tdda_status tdda_profile_gram_schmidt(tdda_model *m, int precision, int nv, int iters, double *ms);
 /* No reference counterpart (measurement support): the damped periodic lattice
  * sums -- the interaction tensor's entries before its FFT, as
  * AProductCore::A_dic_generator forms them (src/AProductCore.cpp:335-349) --

@@ -142,3 +142,15 @@ def test_recycling_rejects_too_short_cycles(sici):
     with pytest.raises(RuntimeError):
         m.setSolver("gmres-dr-recycle", degree=1, restart=10, deflate=0)
     m.setSolver("gmres-dr-recycle", degree=1, restart=12, deflate=6)
+
+
+def test_profile_gram_schmidt(sici):
+    """The Gram-Schmidt timing entry point runs both kernels in both precisions
+    (odd and even vector lengths: packed and element-wise paths)."""
+    from dda_model import DDAModel
+
+    for shape in ((16, 16, 8), (7, 5, 3)):
+        m = DDAModel(**model_args(*shape, sici, seed=2), precision="mixed")
+        for prec in ("mixed", "complex128"):
+            a, b = m.profile_gram_schmidt(prec, nv=9, iters=3)
+            assert 0.0 < a < 100.0 and 0.0 < b < 100.0, (shape, prec, a, b)

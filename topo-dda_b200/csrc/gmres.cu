@@ -1439,6 +1439,45 @@ tdda_status pgmres_solve(const RefineWork<C> &w, GmresWork<C> &gw, const double2
     return TDDA_OK;
 }
 
+// Timing of the two Gram-Schmidt kernels (CUDA events on stream s) on a
+// scratch basis of nv + 1 vectors of n3 elements: ms[0] = projections and norm
+// against nv vectors (k_multidot_bulk or its element-wise variant, without the
+// host read-back), ms[1] = the update and normalisation.  The vectors hold a
+// constant pattern; the time does not depend on the values.
+template <typename C> tdda_status profile_gram_schmidt(long long n3, int nv, int iters, cudaStream_t s, double *ms) {
+    GmresWork<C> gw;
+    tdda_status st = gw.init(n3, 1, nv, 1, 0);
+    if (st != TDDA_OK) {
+        gw.release();
+        return st;
+    }
+    const size_t vec = sizeof(C) * (size_t)n3;
+    TDDA_CUDA_TRY(cudaMemsetAsync(gw.V, 0x3c, vec * (nv + 1), s));   // finite floats and doubles
+    TDDA_CUDA_TRY(cudaMemsetAsync(gw.coef, 0, sizeof(double2) * (nv + 1), s));
+    C *w = basis(gw, nv);
+    cudaEvent_t e[4];
+    for (auto &x : e) TDDA_CUDA_TRY(cudaEventCreate(&x));
+    multidot(gw, nv, w, gw.h, s);            // warm-up
+    gs_update_scale(gw, nv, (const double2 *)gw.coef, w, s);
+    TDDA_CUDA_TRY(cudaEventRecord(e[0], s));
+    for (int i = 0; i < iters; ++i) multidot(gw, nv, w, gw.h, s);
+    TDDA_CUDA_TRY(cudaEventRecord(e[1], s));
+    TDDA_CUDA_TRY(cudaEventRecord(e[2], s));
+    for (int i = 0; i < iters; ++i) gs_update_scale(gw, nv, (const double2 *)gw.coef, w, s);
+    TDDA_CUDA_TRY(cudaEventRecord(e[3], s));
+    TDDA_CUDA_TRY(cudaEventSynchronize(e[3]));
+    float a = 0.f, b = 0.f;
+    TDDA_CUDA_TRY(cudaEventElapsedTime(&a, e[0], e[1]));
+    TDDA_CUDA_TRY(cudaEventElapsedTime(&b, e[2], e[3]));
+    ms[0] = a / iters;
+    ms[1] = b / iters;
+    for (auto &x : e) cudaEventDestroy(x);
+    gw.release();
+    return TDDA_OK;
+}
+
+template tdda_status profile_gram_schmidt<float2>(long long, int, int, cudaStream_t, double *);
+template tdda_status profile_gram_schmidt<double2>(long long, int, int, cudaStream_t, double *);
 template struct GmresWork<float2>;
 template struct GmresWork<double2>;
 template tdda_status pgmres_solve<float2>(const RefineWork<float2> &, GmresWork<float2> &, const double2 *, double2 *,

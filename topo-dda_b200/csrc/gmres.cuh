@@ -70,6 +70,11 @@ template <typename C>
 tdda_status pgmres_solve(const RefineWork<C> &w, GmresWork<C> &gw, const double2 *B, double2 *X, int nrhs,
                          bool x0_zero, int max_iter, double tol, const GmresOptions &o, tdda_solve_info *info);
 
+// Mean time of the Gram-Schmidt projection kernel (ms[0], with the block-sum
+// kernel) and of the update kernel (ms[1]) against nv basis vectors of n3
+// elements, on a scratch basis (measurement support).
+template <typename C> tdda_status profile_gram_schmidt(long long n3, int nv, int iters, cudaStream_t s, double *ms);
+
 // --- host linear algebra of the polynomial ----------------------------------
 // Eigenvalues of the n x n upper-Hessenberg matrix H (column-major, ld;
 // destroyed) by shifted QR; false if it did not converge.

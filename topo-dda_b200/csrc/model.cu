@@ -1379,6 +1379,13 @@ tdda_status tdda_profile_matvec(tdda_model *m, int precision, int nrhs, int iter
     return profile_apply<float2>(m->op32, m->kv32.r, m->kv32.p, m->al32, nrhs, iters, m->stream, ms_matvec, ms_pass);
 }
 
+tdda_status tdda_profile_gram_schmidt(tdda_model *m, int precision, int nv, int iters, double *ms) {
+    if (!m || !ms || nv < 1 || nv > 1024 || iters < 1) return bad("bad argument");
+    if (precision == 0) return profile_gram_schmidt<double2>(3 * m->nbox, nv, iters, m->stream, ms);
+    if (precision == 1) return profile_gram_schmidt<float2>(3 * m->nbox, nv, iters, m->stream, ms);
+    return bad("precision must be 0 or 1");
+}
+
 long long tdda_kernel_launches(void) { return launches_total(); }
 
 tdda_status tdda_set_precision(tdda_model *m, int precision) {

@@ -275,6 +275,14 @@ class DDAModel:
                                                  int(nrhs), int(iters), ctypes.byref(tot), passes))
         return tot.value, [passes[0], passes[1], passes[2]]
 
+    def profile_gram_schmidt(self, precision="mixed", nv=25, iters=20):
+        """Device time (ms) of one GMRES projection pass and of one update pass
+        against nv basis vectors of this model's size (scratch basis)."""
+        ms = (ctypes.c_double * 2)()
+        _lib.check(self._lib.tdda_profile_gram_schmidt(self._handle, 0 if precision in ("complex128", "c128") else 1,
+                                                       int(nv), int(iters), ms))
+        return ms[0], ms[1]
+
     def setPrecision(self, precision):
         """Switch later solves between "complex128" and "mixed" (mixed models only)."""
         _lib.check(self._lib.tdda_set_precision(self._handle, _PRECISIONS[precision]))

@@ -177,6 +177,8 @@ SIGNATURES = {
     "tdda_set_precision": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "tdda_set_preconditioner": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "tdda_set_time_limit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
+    "tdda_profile_gram_schmidt": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                  ctypes.POINTER(ctypes.c_double)]),
     "tdda_set_solver": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "tdda_filter_update": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_int64, ctypes.c_int, ctypes.c_int]),
     "tdda_filter_gradients": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_int64, ctypes.c_int, ctypes.c_int, _dp]),
