@@ -21,6 +21,15 @@ constexpr int kGsChunk = 8;   // basis vectors per multi-dot CTA
 // refinement step that starts from a recycled space adds one)
 constexpr int kMaxAug = 4;
 
+// The nv basis vectors split into nch = gridDim.y chunks of near-equal size
+// (at most kGsChunk each, the first nv % nch one larger), so that the CTAs of
+// every chunk stream about the same bytes: chunk c holds [i0, i0 + nb).
+__device__ __forceinline__ void chunk_of(int nv, int c, int nch, int &i0, int &nb) {
+    const int base = nv / nch, rem = nv % nch;
+    nb = base + (c < rem ? 1 : 0);
+    i0 = c * base + min(c, rem);
+}
+
 template <int NV> __device__ __forceinline__ void block_sum_v(double2 (&v)[NV], double2 *sm) {
     // sm: NV * (kGsThreads / 32) double2
 #pragma unroll
@@ -103,8 +112,9 @@ __global__ void __launch_bounds__(kGsThreads, 2) k_multidot_bulk(long long np, i
     __shared__ __align__(8) unsigned long long full[kBdStages];
     __shared__ double2 sm[(kGsChunk + 1) * (kGsThreads / 32)];
     PT *tiles = reinterpret_cast<PT *>(bd_smem);   // [stage][vector (w last)][kBdTile]
-    const int k = blockIdx.z, i0 = blockIdx.y * kGsChunk;
-    const int nb = min(kGsChunk, nv - i0);
+    const int k = blockIdx.z;
+    int i0, nb;
+    chunk_of(nv, blockIdx.y, gridDim.y, i0, nb);
     const bool norm = no > nv && blockIdx.y == 0;
     const long long ntiles = (np + kBdTile - 1) / kBdTile;
     const PT *wk = w + (size_t)k * rstr;
@@ -222,8 +232,9 @@ __global__ void __launch_bounds__(kGsThreads) k_multidot_e(long long n, int nv, 
                                                            double2 *__restrict__ part) {
     pdl_wait();
     __shared__ double2 sm[(kGsChunk + 1) * (kGsThreads / 32)];
-    const int k = blockIdx.z, i0 = blockIdx.y * kGsChunk;
-    const int nb = min(kGsChunk, nv - i0);
+    const int k = blockIdx.z;
+    int i0, nb;
+    chunk_of(nv, blockIdx.y, gridDim.y, i0, nb);
     const bool norm = no > nv && blockIdx.y == 0;
     double2 acc[kGsChunk + 1];
 #pragma unroll
@@ -1176,7 +1187,8 @@ tdda_status pgmres_solve(const RefineWork<C> &w, GmresWork<C> &gw, const double2
     const size_t vstr = (size_t)n * nrhs;
     const int max_refine = 60;
     for (int outer = 0; outer <= max_refine; ++outer) {
-        tdda_status st = residual_c128(*w.op64, w.al64, B, X, w.Rm, w.st_res, nrhs, s, w.dstride);
+        tdda_status st = residual_c128(*w.op64, w.al64, B, X, w.Rm, w.st_res, nrhs, s, w.dstride,
+                                        w.post.eres != nullptr ? &w.post : nullptr);
         if (st != TDDA_OK) return st;
         TDDA_CUDA_TRY(cudaMemcpyAsync(w.st_res_host, w.st_res, sizeof(SolverState) * nrhs, cudaMemcpyDeviceToHost, s));
         TDDA_CUDA_TRY(cudaStreamSynchronize(s));

@@ -821,14 +821,16 @@ template <typename C> struct EpiPoly : EpiBase<C> {
 
 // r = B - (A x0 + al o x0); r0 = r;  sums: r0.r, ||B||^2   src/DDAModel.cpp:925-928
 template <typename C> struct EpiInit : EpiBase<C> {
-    static constexpr int NQ = 2;
+    static constexpr int NQ = 3;
     const C *x0, *b, *al;
     C *r, *r0;
     SolverState *st;
+    ResidualPost post;   // E_int and the objective sum of right-hand side 0 (off when post.eres is null)
     __device__ bool skip(int rhs) const { return false; }
     __device__ void apply(int rhs, int c, long long cell, C conv, double2 *acc) const {
         size_t i = this->idx(rhs, c, cell);
-        C ax = this->masked(rhs, cell, conv) + __ldg(al + this->didx(rhs, cell)) * __ldg(x0 + i);
+        const C alx = __ldg(al + this->didx(rhs, cell)) * __ldg(x0 + i);
+        C ax = this->masked(rhs, cell, conv) + alx;
         C bb = __ldg(b + i);
         C v = bb - ax;
         r[i] = v;
@@ -838,9 +840,19 @@ template <typename C> struct EpiInit : EpiBase<C> {
         acc[0].x += d.x;
         acc[0].y += d.y;
         acc[1].x += bd.x * bd.x + bd.y * bd.y;
+        if (post.eres != nullptr && rhs == 0) {
+            const double2 a = to_d(alx);
+            const double2 e = __ldg(post.diel + cell);
+            post.eres[(size_t)c * this->nbox + cell] = cdiv(a, make_double2((2.0 + e.x) / 3.0, e.y / 3.0));
+            if (post.mask == nullptr || __ldg(post.mask + cell) != 0) {
+                const double m = hypot(a.x, a.y);
+                acc[2].x += post.q == 2 ? m * m : pow(m, (double)post.q);
+            }
+        }
     }
     __device__ void operator()(int rhs, const double2 *s) const {
         SolverState &S = st[rhs];
+        S.post_sum = s[2].x;
         S.rho = s[0];
         S.rho_prev = make_double2(0.0, 0.0);
         S.enorm = sqrt(s[1].x);
@@ -1792,7 +1804,8 @@ template tdda_status profile_apply<float2>(ConvOperator<float2> &, const float2 
                                            int, cudaStream_t, double *, double *);
 
 tdda_status residual_c128(ConvOperator<double2> &op, const double2 *al, const double2 *B, const double2 *X,
-                          double2 *R, SolverState *st, int nrhs, cudaStream_t s, size_t dstride) {
+                          double2 *R, SolverState *st, int nrhs, cudaStream_t s, size_t dstride,
+                          const ResidualPost *post) {
     ConvGeom g;
     if (nrhs > op.nrhs_cap || !geom_for(op, nrhs, g)) { set_error("batch does not fit"); return TDDA_ERR_UNSUPPORTED; }
     ProLoad<double2> pro{};
@@ -1801,6 +1814,7 @@ tdda_status residual_c128(ConvOperator<double2> &op, const double2 *al, const do
     epi.nbox = g.nbox; epi.mask = op.mask; epi.part = op.partials; epi.counter = op.counters;
     epi.pstride = (size_t)op.partial_cap; epi.x0 = X; epi.b = B; epi.al = al; epi.r = R; epi.r0 = R; epi.st = st;
     epi.dstride = dstride;
+    if (post != nullptr) epi.post = *post;
     run_conv(op, g, nrhs, pro, epi, nullptr, s);
     TDDA_CUDA_TRY(cudaGetLastError());
     return TDDA_OK;

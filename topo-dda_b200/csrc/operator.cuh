@@ -25,6 +25,19 @@ struct SolverState {
     double best_err;
     int pending;        // fused steps: the last iteration's P update is not applied yet
     int pad_;
+    double post_sum;    // true-residual evaluation with ResidualPost: sum over dipole cells of |al x_c|^q
+};
+
+// Post-processing fused into the true-residual evaluation of right-hand side 0
+// (the last kernel of a refinement solve evaluates the final solution X): the
+// internal field E_int = al X / ((2 + eps) / 3) (DDAModel::solveElectricField's
+// EResult, src/DDAModel.cpp:1153-1192) and the IntegratedE sum
+// S = sum over dipole cells of sum_c |al X_c|^q (src/ObjDDAModel.cpp:103-218).
+struct ResidualPost {
+    double2 *eres = nullptr;              // [3][nbox] in the box layout, or nullptr: off
+    const double2 *diel = nullptr;        // permittivity per cell
+    const unsigned char *mask = nullptr;  // dipole cells (nullptr: every cell)
+    int q = 2;
 };
 
 // Geometry + device buffers of one operator instance (one precision).
@@ -96,9 +109,11 @@ tdda_status apply_external_scratch(const ConvOperator<C> &op, C *T_ext, const C 
                                    cudaStream_t s);
 
 // R = B - (A + diag al) X in complex128 (one fused convolution); st receives
-// enorm = ||B|| and err = ||R|| / ||B|| per right-hand side.
+// enorm = ||B|| and err = ||R|| / ||B|| per right-hand side; with post
+// (eres != nullptr) also E_int of X[0] and st[0].post_sum.
 tdda_status residual_c128(ConvOperator<double2> &op, const double2 *al, const double2 *B, const double2 *X,
-                          double2 *R, SolverState *st, int nrhs, cudaStream_t s, size_t dstride = 0);
+                          double2 *R, SolverState *st, int nrhs, cudaStream_t s, size_t dstride = 0,
+                          const ResidualPost *post = nullptr);
 
 // Times `iters` back-to-back applications of the operator, then each pass
 // alone, with CUDA events on stream s: ms_total = mean per application,

@@ -73,7 +73,8 @@ tdda_status refine_solve(const RefineWork<C> &w, const double2 *B, double2 *X, i
     const int kInnerStall = 150;
     double *h = w.h_part;
     for (int outer = 0; outer <= max_refine; ++outer) {
-        tdda_status st = residual_c128(*w.op64, w.al64, B, X, w.Rm, w.st_res, nrhs, s, w.dstride);
+        tdda_status st = residual_c128(*w.op64, w.al64, B, X, w.Rm, w.st_res, nrhs, s, w.dstride,
+                                        w.post.eres != nullptr ? &w.post : nullptr);
         if (st != TDDA_OK) return st;
         TDDA_CUDA_TRY(cudaMemcpyAsync(w.st_res_host, w.st_res, sizeof(SolverState) * nrhs, cudaMemcpyDeviceToHost, s));
         TDDA_CUDA_TRY(cudaStreamSynchronize(s));

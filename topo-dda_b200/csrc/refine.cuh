@@ -26,6 +26,10 @@ template <typename C> struct RefineWork {
     int graph_steps = 0;                    // inner BiCGSTAB: iterations per CUDA graph (0: none)
     double time_limit_s = 0.0;              // inner BiCGSTAB: device-side time limit (0: none)
     cudaStream_t s = nullptr;
+    // E_int and the objective sum of X[0], fused into every true-residual
+    // evaluation (the last one evaluates the returned solution); off when
+    // post.eres is null
+    ResidualPost post{};
 };
 
 // Solves (A + diag al) X = B to a TRUE relative residual <= tol per
