@@ -206,6 +206,40 @@ tdda_status tdda_design_forward_device(int nx, int ny, int nz, double radius, do
 tdda_status tdda_design_backward_device(int nx, int ny, int nz, double radius, double beta, double eta,
                                         const double *filtered_dev, const double *grad_rho_dev, double *grad_raw_dev,
                                         double *scratch_dev, void *stream);
+
+/* The topology-optimisation loop on the device (calculation_scripts/
+ * TopoOptCalculation.py:165-209), each piece in the model's or the caller's
+ * device memory:
+ * - free parameters -> per-dipole densities through the model's parameter map
+ *   (src/DDAModel.cpp:163-247; feed rho_dev to tdda_set_densities_device);
+ * - per-dipole gradient -> per-parameter gradient, each parameter's dipoles
+ *   added one at a time in dipole order (the host loop's scatter-add);
+ * - a forward solve that starts from the model's current polarisation (the
+ *   warm start the host loop makes by passing the previous P back in);
+ * - the update: penalty and its gradient (binarizers.py:5-34), the penalised
+ *   gradient, Adam (optimizers.py:3-23, bias correction inside the moving
+ *   averages), the clipped ascent step, every operation rounded on its own in
+ *   the order the host loop evaluates it.  penalty_out / penalty_grad_out
+ *   (NFpara doubles, the reference's per-iteration penalty files) and
+ *   penalty_mean_out (one double) may be null. */
+typedef struct {
+    int penalty;                       /* 0 parabolic, 1 gaussian, 2 triangular */
+    double sigma, mu;                  /* gaussian */
+    double slope;                      /* triangular */
+    double coeff, one_minus_coeff;     /* penalty coefficient c of this iteration and 1 - c */
+    double step;                       /* step size */
+    double beta1, beta2;               /* Adam */
+    double one_minus_beta1, one_minus_beta2;
+    double bias1, bias2;               /* 1 - beta1^(t+1), 1 - beta2^(t+1) at timestep t */
+} tdda_ascent_step;
+tdda_status tdda_params_to_densities_device(tdda_model *m, const double *params_dev, double *rho_dev,
+                                           void *stream);
+tdda_status tdda_densities_to_params_device(tdda_model *m, const double *grad_dev, double *grad_params_dev,
+                                           void *stream);
+tdda_status tdda_solve_electric_field_warm(tdda_model *m, int max_iter, double tol, tdda_solve_info *info);
+tdda_status tdda_ascent_step_device(int64_t n, double *params, double *adam_v, double *adam_s,
+                                    const double *grad_obj, const tdda_ascent_step *cfg, double *penalty_out,
+                                    double *penalty_grad_out, double *penalty_mean_out, void *stream);
 /* Observation-patch objective (no reference counterpart; the nearest is
  * ObjPointEDDAModel, src/ObjDDAModel.cpp:20-100, and the off-structure branch
  * of DDAModel::solve_E, src/DDAModel.cpp:1154-1179): points xyz[3*nobs] in grid

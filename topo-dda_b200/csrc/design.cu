@@ -13,6 +13,7 @@
 // densities are in dipole order (x fastest), the order the model takes.
 // Products and sums are rounded one at a time in the offset order
 // dx, dy, dz ascending, as a plain elementwise evaluation does.
+#include <algorithm>
 #include <cmath>
 #include <string>
 
@@ -169,3 +170,95 @@ extern "C" tdda_status tdda_design_backward_device(int nx, int ny, int nz, doubl
     TDDA_CUDA_TRY(cudaGetLastError());
     return TDDA_OK;
 }
+
+// ----------------------------------------------------------------------------
+// One iteration's update of the topology-optimisation loop on the device
+// (calculation_scripts/TopoOptCalculation.py:165-209): penalty and its
+// gradient (python_bindings/dda_model/binarizers.py:5-34), the penalised
+// gradient, Adam with its bias correction inside the moving averages
+// (optimizers.py:3-23), the clipped ascent step.  Every product, sum, quotient
+// and square root is rounded on its own, in the order the reference's numpy
+// expressions evaluate, so the update is the host loop's to the last bit
+// (exp in the gaussian penalty aside).
+// ----------------------------------------------------------------------------
+namespace tdda {
+
+__device__ __forceinline__ void penalty_of(const tdda_ascent_step &c, double x, double &pen, double &pg) {
+    if (c.penalty == 0) {            // parabolic: x - x^2, 1 - 2x
+        pen = __dsub_rn(x, __dmul_rn(x, x));
+        pg = __dsub_rn(1.0, __dmul_rn(2.0, x));
+    } else if (c.penalty == 1) {     // gaussian
+        const double t = __ddiv_rn(__dsub_rn(x, c.mu), c.sigma);
+        pen = __dmul_rn(c.sigma, exp(__dadd_rn(-__ddiv_rn(__dmul_rn(t, t), 2.0), 0.5)));
+        pg = __ddiv_rn(__dmul_rn(-__dsub_rn(x, c.mu), pen), __dmul_rn(c.sigma, c.sigma));
+    } else {                         // triangular
+        pen = x > 0.5 ? __dsub_rn(c.slope, __dmul_rn(c.slope, x)) : __dmul_rn(c.slope, x);
+        pg = x > 0.5 ? -c.slope : c.slope;
+    }
+}
+
+__global__ void k_ascent(long long n, double *__restrict__ x, double *__restrict__ V, double *__restrict__ S,
+                         const double *__restrict__ gobj, tdda_ascent_step c, double *__restrict__ pen_out,
+                         double *__restrict__ pg_out) {
+    for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += (long long)gridDim.x * blockDim.x) {
+        const double xj = x[j];
+        double pen, pg;
+        penalty_of(c, xj, pen, pg);
+        if (pen_out) pen_out[j] = pen;
+        if (pg_out) pg_out[j] = pg;
+        const double g = __dsub_rn(__dmul_rn(c.one_minus_coeff, gobj[j]), __dmul_rn(c.coeff, pg));
+        const double v = __dadd_rn(__dmul_rn(c.beta1, V[j]), __ddiv_rn(__dmul_rn(c.one_minus_beta1, g), c.bias1));
+        const double sq = __dadd_rn(__dmul_rn(c.beta2, S[j]),
+                                    __ddiv_rn(__dmul_rn(__dmul_rn(c.one_minus_beta2, g), g), c.bias2));
+        V[j] = v;
+        S[j] = sq;
+        const double stp = __ddiv_rn(v, __dadd_rn(__dsqrt_rn(sq), 1e-8));
+        x[j] = fmin(fmax(__dadd_rn(xj, __dmul_rn(c.step, stp)), 0.0), 1.0);
+    }
+}
+
+// mean of pen[0..n) by one CTA: per-thread strided sums, then a fixed tree
+__global__ void k_mean(long long n, const double *__restrict__ v, double *__restrict__ out) {
+    __shared__ double sm[256];
+    double s = 0.0;
+    for (long long j = threadIdx.x; j < n; j += blockDim.x) s += v[j];
+    sm[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) sm[threadIdx.x] += sm[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = sm[0] / (double)n;
+}
+
+}  // namespace tdda
+
+extern "C" tdda_status tdda_ascent_step_device(int64_t n, double *params, double *adam_v, double *adam_s,
+                                               const double *grad_obj, const tdda_ascent_step *cfg,
+                                               double *penalty_out, double *penalty_grad_out,
+                                               double *penalty_mean_out, void *stream) {
+    using namespace tdda;
+    if (n < 1 || !params || !adam_v || !adam_s || !grad_obj || !cfg) {
+        set_error("tdda_ascent_step_device: bad argument");
+        return TDDA_ERR_BAD_ARG;
+    }
+    if (cfg->penalty < 0 || cfg->penalty > 2) {
+        set_error("penalty must be 0 (parabolic), 1 (gaussian) or 2 (triangular)");
+        return TDDA_ERR_BAD_ARG;
+    }
+    if (penalty_mean_out != nullptr && penalty_out == nullptr) {
+        set_error("the penalty mean needs penalty_out");
+        return TDDA_ERR_BAD_ARG;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    const unsigned nb = (unsigned)std::min<long long>((n + 255) / 256, 148 * 8);
+    count_launches(1);
+    k_ascent<<<nb, 256, 0, s>>>(n, params, adam_v, adam_s, grad_obj, *cfg, penalty_out, penalty_grad_out);
+    if (penalty_mean_out) {
+        count_launches(1);
+        k_mean<<<1, 256, 0, s>>>(n, penalty_out, penalty_mean_out);
+    }
+    TDDA_CUDA_TRY(cudaGetLastError());
+    return TDDA_OK;
+}
+

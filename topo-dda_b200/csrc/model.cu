@@ -451,6 +451,9 @@ struct tdda_model {
     double2 *sc64 = nullptr, *alS64 = nullptr;
     float2 *sc32 = nullptr, *alS32 = nullptr;
     double *d_grad = nullptr;              // per-cell gradient scratch
+    // the parameter map on the device (built on first use): parameter of each
+    // dipole, and each parameter's dipoles in dipole order (CSR)
+    int32_t *d_pmap = nullptr, *d_pptr = nullptr, *d_pidx = nullptr;
     unsigned *d_flag = nullptr, *h_flag = nullptr;  // density check count (device, pinned)
     SolverState *st_res = nullptr, *st_res_host = nullptr;
     double *d_part = nullptr, *h_part = nullptr;
@@ -485,7 +488,7 @@ struct tdda_model {
         gw32.release();
         void *bufs[] = {d_cell, d_mask, d_rho,  al,  diel, al32,  Einc, P,     Eres,  ext,   bufB,     bufX,
                         Rm,     R32,    D32,    st_res, d_part, R64, D64,  sc64, alS64, sc32, alS32, d_obs,
-                        Gobs,   Einc_obs, Eobs, d_grad, d_flag};
+                        Gobs,   Einc_obs, Eobs, d_grad, d_flag, d_pmap, d_pptr, d_pidx};
         for (void *b : bufs) cudaFree(b);
         cudaFreeHost(h_flag);
         cudaFreeHost(st_res_host);
@@ -1383,6 +1386,43 @@ static tdda_status cells_to_host(tdda_model *m, const double *cells, double *out
     return TDDA_OK;
 }
 
+// rho[i] = params[pmap[i]] (free parameters -> per-dipole densities)
+__global__ void k_param_gather(long long n, const int32_t *__restrict__ pmap, const double *__restrict__ params,
+                               double *__restrict__ rho) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        rho[i] = params[pmap[i]];
+}
+
+// out[j] = sum of g over parameter j's dipoles, added one at a time in dipole
+// order (the order of a sequential scatter-add over the dipoles)
+__global__ void k_param_sum(long long np, const int32_t *__restrict__ ptr, const int32_t *__restrict__ idx,
+                            const double *__restrict__ g, double *__restrict__ out) {
+    for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < np; j += (long long)gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int k = ptr[j]; k < ptr[j + 1]; ++k) s = __dadd_rn(s, g[idx[k]]);
+        out[j] = s;
+    }
+}
+
+static tdda_status ensure_pmap(tdda_model *m) {
+    if (m->d_pmap != nullptr) return TDDA_OK;
+    const int np = m->NFpara;
+    std::vector<int32_t> ptr(np + 1, 0), idx(m->N), map(m->geometryPara.begin(), m->geometryPara.end());
+    for (int i = 0; i < m->N; ++i) ptr[map[i] + 1] += 1;
+    for (int j = 0; j < np; ++j) ptr[j + 1] += ptr[j];
+    std::vector<int32_t> fill(ptr.begin(), ptr.end() - 1);
+    for (int i = 0; i < m->N; ++i) idx[fill[map[i]]++] = i;
+    int32_t *a = nullptr, *b = nullptr, *c = nullptr;
+    TDDA_CUDA_TRY(cudaMalloc(&a, sizeof(int32_t) * m->N));
+    TDDA_CUDA_TRY(cudaMalloc(&b, sizeof(int32_t) * (np + 1)));
+    TDDA_CUDA_TRY(cudaMalloc(&c, sizeof(int32_t) * m->N));
+    TDDA_CUDA_TRY(cudaMemcpy(a, map.data(), sizeof(int32_t) * m->N, cudaMemcpyHostToDevice));
+    TDDA_CUDA_TRY(cudaMemcpy(b, ptr.data(), sizeof(int32_t) * (np + 1), cudaMemcpyHostToDevice));
+    TDDA_CUDA_TRY(cudaMemcpy(c, idx.data(), sizeof(int32_t) * m->N, cudaMemcpyHostToDevice));
+    m->d_pmap = a; m->d_pptr = b; m->d_pidx = c;
+    return TDDA_OK;
+}
+
 static tdda_status cells_to_device(tdda_model *m, const double *cells, double *out_dev, cudaStream_t user) {
     count_launches(1);
     k_cell_to_dipole<<<grid_for(m->N), 256, 0, m->stream>>>(m->N, m->d_cell, cells, out_dev);
@@ -1404,6 +1444,45 @@ tdda_status tdda_gradient_densities_device(tdda_model *m, int max_iter, double t
     TRY(join_streams((cudaStream_t)stream, m->stream));
     TRY(gradient_cells(m, max_iter, tol, info));
     return cells_to_device(m, m->d_grad, grad_dev, (cudaStream_t)stream);
+}
+
+tdda_status tdda_params_to_densities_device(tdda_model *m, const double *params_dev, double *rho_dev,
+                                           void *stream) {
+    if (!m || !params_dev || !rho_dev) return bad("null argument");
+    TRY(ensure_pmap(m));
+    cudaStream_t user = (cudaStream_t)stream;
+    TRY(join_streams(user, m->stream));
+    count_launches(1);
+    k_param_gather<<<grid_for(m->N), 256, 0, m->stream>>>(m->N, m->d_pmap, params_dev, rho_dev);
+    TDDA_CUDA_TRY(cudaGetLastError());
+    return join_streams(m->stream, user);
+}
+
+tdda_status tdda_densities_to_params_device(tdda_model *m, const double *grad_dev, double *grad_params_dev,
+                                           void *stream) {
+    if (!m || !grad_dev || !grad_params_dev) return bad("null argument");
+    TRY(ensure_pmap(m));
+    cudaStream_t user = (cudaStream_t)stream;
+    TRY(join_streams(user, m->stream));
+    count_launches(1);
+    k_param_sum<<<grid_for(m->NFpara), 256, 0, m->stream>>>(m->NFpara, m->d_pptr, m->d_pidx, grad_dev,
+                                                            grad_params_dev);
+    TDDA_CUDA_TRY(cudaGetLastError());
+    return join_streams(m->stream, user);
+}
+
+tdda_status tdda_solve_electric_field_warm(tdda_model *m, int max_iter, double tol, tdda_solve_info *info) {
+    if (!m) return bad("null model");
+    tdda_solve_info inf{};
+    TRY(solve_internal(m, m->Einc, m->P, 1, false, max_iter, tol, &inf));
+    if (m->post_gen != m->gen) {
+        count_launches(1);
+        k_eresult<<<grid_for(3 * m->nbox), 256, 0, m->stream>>>(m->nbox, m->P, m->al, m->diel, m->Eres);
+        TDDA_CUDA_TRY(cudaGetLastError());
+    }
+    TDDA_CUDA_TRY(cudaStreamSynchronize(m->stream));
+    if (info) *info = inf;
+    return TDDA_OK;
 }
 
 tdda_status tdda_profile_matvec(tdda_model *m, int precision, int nrhs, int iters, double *ms_matvec,

@@ -130,6 +130,22 @@ class DDAModel:
         self.last_solve = info.as_dict()
         return None
 
+    def solveElectricFieldWarm(self, BGS_MAX_ITER, BGS_MAX_ERROR):
+        """solveElectricField starting from the model's current polarisation
+        (already on the device: no host copy of the initial guess)."""
+        info = _lib.SolveInfo()
+        _lib.check(self._lib.tdda_solve_electric_field_warm(self._handle, int(BGS_MAX_ITER), float(BGS_MAX_ERROR),
+                                                            ctypes.byref(info)))
+        self.last_solve = info.as_dict()
+
+    def paramsToDensitiesDevice(self, params_ptr, rho_ptr, stream=None):
+        """rho[i] = params[parameterMap()[i]] on device arrays (NFpara -> N doubles)."""
+        _lib.check(self._lib.tdda_params_to_densities_device(self._handle, params_ptr, rho_ptr, stream))
+
+    def densitiesToParamsDevice(self, grad_ptr, out_ptr, stream=None):
+        """Per-parameter sums of a per-dipole gradient on device arrays (N -> NFpara)."""
+        _lib.check(self._lib.tdda_densities_to_params_device(self._handle, grad_ptr, out_ptr, stream))
+
     def calculateObjective(self):
         """src/DDAModel.cpp:870-872 (IntegratedE)."""
         out = ctypes.c_double()

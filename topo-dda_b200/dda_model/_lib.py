@@ -56,6 +56,15 @@ class Params(ctypes.Structure):
     ]
 
 
+class AscentStep(ctypes.Structure):
+    """tdda_ascent_step (include/tdda.h)."""
+    _fields_ = [("penalty", ctypes.c_int), ("sigma", ctypes.c_double), ("mu", ctypes.c_double),
+                ("slope", ctypes.c_double), ("coeff", ctypes.c_double), ("one_minus_coeff", ctypes.c_double),
+                ("step", ctypes.c_double), ("beta1", ctypes.c_double), ("beta2", ctypes.c_double),
+                ("one_minus_beta1", ctypes.c_double), ("one_minus_beta2", ctypes.c_double),
+                ("bias1", ctypes.c_double), ("bias2", ctypes.c_double)]
+
+
 class SolveInfo(ctypes.Structure):
     _fields_ = [
         ("iterations", ctypes.c_int),
@@ -195,6 +204,15 @@ SIGNATURES = {
                                                    ctypes.c_double, ctypes.c_double, ctypes.c_void_p,
                                                    ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                                    ctypes.c_void_p]),
+    "tdda_params_to_densities_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                                       ctypes.c_void_p]),
+    "tdda_densities_to_params_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                                       ctypes.c_void_p]),
+    "tdda_solve_electric_field_warm": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_double,
+                                                      ctypes.POINTER(SolveInfo)]),
+    "tdda_ascent_step_device": (ctypes.c_int, [ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                               ctypes.c_void_p, ctypes.POINTER(AscentStep), ctypes.c_void_p,
+                                               ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "tdda_set_observation_points": (ctypes.c_int, [ctypes.c_void_p, _ip, ctypes.c_int64]),
     "tdda_observation_field": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_int64]),
     "tdda_patch_objective": (ctypes.c_int, [ctypes.c_void_p, _dp]),

@@ -19,6 +19,7 @@ for formula (they define the optimisation trajectory).
 """
 from __future__ import annotations
 
+import ctypes
 import math
 import os
 from dataclasses import dataclass, field
@@ -188,3 +189,91 @@ class TopologyOptimization:
         if self.data_path:
             dio.save_summary(self.data_path, self.history, self.penalty_type, self.penalty_config)
         return self.history
+
+
+_PENALTY_KIND = {"parabolic": 0, "gaussian": 1, "triangular": 2}
+
+
+class DeviceTopologyOptimization(TopologyOptimization):
+    """The same loop with its state on the GPU: the free parameters, Adam's
+    moving averages, the per-dipole and per-parameter gradients and the
+    penalties live in device memory.  Per iteration: parameters -> densities
+    through the parameter map, a forward solve warm-started from the model's
+    own polarisation, the objective (computed by the solve's last kernel), the
+    exact adjoint gradient into device memory, its per-parameter sums, and the
+    update (penalty, penalised gradient, Adam, clipped step) in one kernel --
+    only scalars (objective, coefficient, mean penalty) reach the host.  Each
+    operation is rounded as the host loop rounds it, so both follow the same
+    trajectory.  The exact adjoint gradient only (gradient="adjoint");
+    data_path files are written from device copies.  The model's parameters
+    are set from the device state when run() ends."""
+
+    def __init__(self, model, *args, device="cuda", **kwargs):
+        super().__init__(model, *args, **kwargs)
+        if self.gradient != "adjoint":
+            raise ValueError("the device loop takes the exact adjoint gradient")
+        if not isinstance(self.opt, Adam):
+            raise ValueError("the device loop runs the reference's Adam")
+        if self.penalty_type not in _PENALTY_KIND:
+            raise ValueError(f"unknown penalty {self.penalty_type!r}")
+        import torch
+
+        self._torch = torch
+        f64 = dict(dtype=torch.float64, device=device)
+        self.params = torch.from_numpy(model.getParameters()).to(**f64)
+        self.V = torch.zeros_like(self.params)
+        self.S = torch.zeros_like(self.params)
+        self.g_obj = torch.zeros_like(self.params)
+        self.pen = torch.zeros_like(self.params)
+        self.pen_grad = torch.zeros_like(self.params)
+        self.pen_mean = torch.zeros(1, **f64)
+        self.rho = torch.zeros(model.N, **f64)
+        self.g_rho = torch.zeros(model.N, **f64)
+        self._first = True
+
+    def step(self, it):
+        from . import _lib
+
+        torch, m, h = self._torch, self.m, self.history
+        stream = torch.cuda.current_stream().cuda_stream
+        m.paramsToDensitiesDevice(self.params.data_ptr(), self.rho.data_ptr(), stream)
+        m.setDensitiesDevice(self.rho.data_ptr(), stream)
+        if self._first or not self.warm_start:
+            m.solveElectricField(None, self.max_iter, self.tol)
+            self._first = False
+        else:
+            m.solveElectricFieldWarm(self.max_iter, self.tol)
+        h.iterations.append(m.last_solve["iterations"])
+        J = m.calculateObjective()
+        h.objective.append(J)
+        m.gradientDensitiesDevice(self.g_rho.data_ptr(), self.max_iter, self.tol, stream)
+        m.densitiesToParamsDevice(self.g_rho.data_ptr(), self.g_obj.data_ptr(), stream)
+        if self.data_path:
+            dio.save_iteration(self.data_path, it, structure=m.getDielectrics(), e_field=m.getElectricField(),
+                               params=self.params.cpu().numpy())
+        coeff = coefficient(self.coeff_type, it, self.coeff_config)
+        h.coefficient.append(coeff)
+        a = self.opt
+        t = a.timestep
+        cfg = self.penalty_config
+        c = _lib.AscentStep(penalty=_PENALTY_KIND[self.penalty_type], sigma=float(cfg.get("sigma", 1.0)),
+                            mu=float(cfg.get("mu", 0.5)), slope=float(cfg.get("slope", 1.0)), coeff=float(coeff),
+                            one_minus_coeff=float(1 - coeff), step=float(self.step_size), beta1=a.beta1,
+                            beta2=a.beta2, one_minus_beta1=1 - a.beta1, one_minus_beta2=1 - a.beta2,
+                            bias1=1 - a.beta1 ** (t + 1), bias2=1 - a.beta2 ** (t + 1))
+        a.timestep += 1
+        _lib.check(_lib.load().tdda_ascent_step_device(
+            self.params.numel(), self.params.data_ptr(), self.V.data_ptr(), self.S.data_ptr(),
+            self.g_obj.data_ptr(), ctypes.byref(c), self.pen.data_ptr(), self.pen_grad.data_ptr(),
+            self.pen_mean.data_ptr(), stream))
+        if self.data_path:
+            dio.save_iteration(self.data_path, it, penalty=self.pen.cpu().numpy(),
+                               penalty_gradient=self.pen_grad.cpu().numpy())
+        h.average_penalty.append(float(self.pen_mean.item()))
+        h.step_size.append(self.step_size)
+        return J
+
+    def run(self, iterations):
+        hist = super().run(iterations)
+        self.m.setParameters(self.params.cpu().numpy())
+        return hist
