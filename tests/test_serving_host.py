@@ -36,3 +36,27 @@ def test_synthetic_stream_shapes_and_arrivals():
     # seeded: the same stream twice
     again = synthetic_stream(n=512, rate=200.0, seed=7)
     assert all(a.lam == b.lam and np.array_equal(a.rho, b.rho) for a, b in zip(reqs, again))
+
+
+def test_per_grid_service_summary():
+    """Per-grid record of a stream: each batch counted once however many
+    requests it merged, service seconds summed per batch."""
+    from dda_model.serving import Result, StreamReport, synthetic_stream
+
+    reqs = synthetic_stream(n=6, rate=100.0, seed=3)
+    shapes = [r.shape for r in reqs]
+    res = []
+    for i, sh in enumerate(shapes):
+        merged = 2 if i < 2 else 1          # the first two requests share one 4-RHS batch
+        res.append(Result(P=None, E=None, info=[{"inner_iterations": 10 + i, "status": "converged",
+                                                 "true_error": 1e-9}] * 2,
+                          batch_rhs=2 * merged, batch_requests=merged, cache_hit=False, worker=0, queue_ms=0.0,
+                          build_ms=0.0, solve_ms=50.0, total_ms=60.0))
+    rep = StreamReport(results=res, requests=reqs, wall_s=1.0)
+    per = rep.per_shape()
+    assert sum(v["requests"] for v in per.values()) == 6
+    assert abs(sum(v["batches"] for v in per.values()) - 5.0) < 1e-12   # 6 requests in 5 batches
+    assert abs(sum(v["solve_s_total"] for v in per.values()) - 0.25) < 1e-12
+    for key, v in per.items():
+        assert key.count("x") == 2
+        assert v["median_batch_solve_ms"] == 50.0
