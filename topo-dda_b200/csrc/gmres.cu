@@ -1458,34 +1458,37 @@ tdda_status pgmres_solve(const RefineWork<C> &w, GmresWork<C> &gw, const double2
 // constant pattern; the time does not depend on the values.
 template <typename C> tdda_status profile_gram_schmidt(long long n3, int nv, int iters, cudaStream_t s, double *ms) {
     GmresWork<C> gw;
-    tdda_status st = gw.init(n3, 1, nv, 1, 0);
-    if (st != TDDA_OK) {
-        gw.release();
-        return st;
-    }
-    const size_t vec = sizeof(C) * (size_t)n3;
-    TDDA_CUDA_TRY(cudaMemsetAsync(gw.V, 0x3c, vec * (nv + 1), s));   // finite floats and doubles
-    TDDA_CUDA_TRY(cudaMemsetAsync(gw.coef, 0, sizeof(double2) * (nv + 1), s));
-    C *w = basis(gw, nv);
-    cudaEvent_t e[4];
-    for (auto &x : e) TDDA_CUDA_TRY(cudaEventCreate(&x));
-    multidot(gw, nv, w, gw.h, s);            // warm-up
-    gs_update_scale(gw, nv, (const double2 *)gw.coef, w, s);
-    TDDA_CUDA_TRY(cudaEventRecord(e[0], s));
-    for (int i = 0; i < iters; ++i) multidot(gw, nv, w, gw.h, s);
-    TDDA_CUDA_TRY(cudaEventRecord(e[1], s));
-    TDDA_CUDA_TRY(cudaEventRecord(e[2], s));
-    for (int i = 0; i < iters; ++i) gs_update_scale(gw, nv, (const double2 *)gw.coef, w, s);
-    TDDA_CUDA_TRY(cudaEventRecord(e[3], s));
-    TDDA_CUDA_TRY(cudaEventSynchronize(e[3]));
-    float a = 0.f, b = 0.f;
-    TDDA_CUDA_TRY(cudaEventElapsedTime(&a, e[0], e[1]));
-    TDDA_CUDA_TRY(cudaEventElapsedTime(&b, e[2], e[3]));
-    ms[0] = a / iters;
-    ms[1] = b / iters;
-    for (auto &x : e) cudaEventDestroy(x);
+    cudaEvent_t e[4] = {nullptr, nullptr, nullptr, nullptr};
+    auto run = [&]() -> tdda_status {
+        tdda_status st = gw.init(n3, 1, nv, 1, 0);
+        if (st != TDDA_OK) return st;
+        const size_t vec = sizeof(C) * (size_t)n3;
+        TDDA_CUDA_TRY(cudaMemsetAsync(gw.V, 0x3c, vec * (nv + 1), s));   // finite floats and doubles
+        TDDA_CUDA_TRY(cudaMemsetAsync(gw.coef, 0, sizeof(double2) * (nv + 1), s));
+        C *w = basis(gw, nv);
+        for (auto &x : e) TDDA_CUDA_TRY(cudaEventCreate(&x));
+        multidot(gw, nv, w, gw.h, s);            // warm-up
+        gs_update_scale(gw, nv, (const double2 *)gw.coef, w, s);
+        TDDA_CUDA_TRY(cudaEventRecord(e[0], s));
+        for (int i = 0; i < iters; ++i) multidot(gw, nv, w, gw.h, s);
+        TDDA_CUDA_TRY(cudaEventRecord(e[1], s));
+        TDDA_CUDA_TRY(cudaEventRecord(e[2], s));
+        for (int i = 0; i < iters; ++i) gs_update_scale(gw, nv, (const double2 *)gw.coef, w, s);
+        TDDA_CUDA_TRY(cudaEventRecord(e[3], s));
+        TDDA_CUDA_TRY(cudaEventSynchronize(e[3]));
+        float a = 0.f, b = 0.f;
+        TDDA_CUDA_TRY(cudaEventElapsedTime(&a, e[0], e[1]));
+        TDDA_CUDA_TRY(cudaEventElapsedTime(&b, e[2], e[3]));
+        ms[0] = a / iters;
+        ms[1] = b / iters;
+        return TDDA_OK;
+    };
+    const tdda_status st = run();
+    for (auto &x : e)
+        if (x) cudaEventDestroy(x);
+    cudaStreamSynchronize(s);   // the scratch basis is freed only after its kernels
     gw.release();
-    return TDDA_OK;
+    return st;
 }
 
 template tdda_status profile_gram_schmidt<float2>(long long, int, int, cudaStream_t, double *);
