@@ -1,5 +1,5 @@
 """Benchmark: DDA solves/s (+ p50/p99 latency), mixed precision vs plain
-complex128, at a 1e-8 relative residual, on configs[2]: a 128x128x32 dipole
+complex128, at a 1e-8 relative residual, on a 128x128x32 dipole
 structure, periodic 128d in x and y.
 
 Workload (one "step" = the solves of both polarisations):
@@ -27,9 +27,9 @@ Under torchrun each rank runs an independent replica (the solves shard by
 request; no collective on the data path) and rank 0 prints one JSON line.
 
 Secondary records in the line: the isolated 128x128x32 structure (the
-previous workload, BiCGSTAB), configs[0] on the GPU (the reference arm's
-workload, for the algorithm-matched ratio), configs[1] (64x64x16, periodic
-64d, complex128), configs[4]'s differentiation step (96x96x24 periodic 96d:
+previous workload, BiCGSTAB), the 16x16x8 isolated workload on the GPU (the reference arm's
+workload, for the algorithm-matched ratio), the 64x64x16 workload (periodic
+64d, complex128), the differentiation step (96x96x24 periodic 96d:
 forward solve + adjoint gradient through the autograd path), the lattice-sum
 kernel, the cuFFT restatement of the reference's A.x, and "serving": the
 request loop of dda_model.serving on 512 requests with seeded Poisson
@@ -263,13 +263,13 @@ def dist_setup():
 # CPU reference arm: the oracle port (the reference has no CPU A.x, and its
 # own build needs Eigen and cuFFT) timed on the host cores
 # ----------------------------------------------------------------------------
-# 16x16x8 dipoles, isolated, rho ~ U[0, 1] per dipole, complex128,
+# the 16x16x8 workload: dipoles isolated, rho ~ U[0, 1] per dipole, complex128,
 # the reference's BiCGSTAB from a zero guess to 1e-8
-C0 = dict(WORKLOAD, nx=16, ny=16, nz=8, period=16, M=0, seed=7)
+SMALL16 = dict(WORKLOAD, nx=16, ny=16, nz=8, period=16, M=0, seed=7)
 
 
 def c0_design():
-    return np.random.default_rng(C0["seed"]).random(C0["nx"] * C0["ny"] * C0["nz"])
+    return np.random.default_rng(SMALL16["seed"]).random(SMALL16["nx"] * SMALL16["ny"] * SMALL16["nz"])
 
 
 class CpuPort:
@@ -314,7 +314,7 @@ class CpuPort:
 
 def run_reference(args):
     """The reference arm: the reference's algorithm on the host cores.  Its
-    headline is measured full solves at configs[0] (16x16x8, where the CPU
+    headline is measured full solves at 16x16x8 (isolated, where the CPU
     finishes them in about a second); on the 128x128x32 periodic workload the
     reference's BiCGSTAB does not reach 1e-8 at all (the GPU arm's line
     records its residual), so that workload gets a measured seconds-per-
@@ -323,23 +323,23 @@ def run_reference(args):
     if rank != 0:
         return 0
     rho0 = c0_design()
-    ports = [CpuPort(C0, rho0, pol) for pol in (0, 1)]
+    ports = [CpuPort(SMALL16, rho0, pol) for pol in (0, 1)]
     cores = ports[0].cores
     steps, infos = [], []
     for k in range(args.warmup + max(args.steps, 5)):
         t = 0.0
         for p in ports:
-            dt, info = p.solve(C0["tol"])
+            dt, info = p.solve(SMALL16["tol"])
             t += dt
             infos.append(info)
         if k >= args.warmup:
             steps.append(t)
     med = statistics.median(steps)
     sps = 2.0 / med
-    # c1 and c2 grids: seconds per complex128 operator application (the unit of
+    # the 64x64x16 and 128x128x32 grids: seconds per complex128 operator application (the unit of
     # work of every solver here), measured on the full grid
-    c1 = dict(WORKLOAD, nx=64, ny=64, nz=16, period=64, M=50)
-    p1 = CpuPort(c1, np.random.default_rng(1).random(64 * 64 * 16), images=False)
+    g64 = dict(WORKLOAD, nx=64, ny=64, nz=16, period=64, M=50)
+    p1 = CpuPort(g64, np.random.default_rng(1).random(64 * 64 * 16), images=False)
     s1 = [p1.per_apply(4) for _ in range(3)]
     w2 = workload(args.small)
     p2 = CpuPort(w2, design(w2), images=False)
@@ -349,10 +349,10 @@ def run_reference(args):
         "steps": len(steps), "warmup": args.warmup, "ms_per_step": med * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
         "data": "synthetic",
-        "config": {"workload": "16x16x8 dipoles (configs[0]), isolated, d=25nm, lambda=542nm, eps 3.5+0.01i, FCD, "
+        "config": {"workload": "16x16x8 dipoles, isolated, d=25nm, lambda=542nm, eps 3.5+0.01i, FCD, "
                                "rho ~ U[0,1] per dipole, x+y polarised (2 RHS/step), the reference's BiCGSTAB "
                                "(unscaled complex128, zero guess) to a 1e-8 recursive residual",
-                   "grid": [16, 16, 8], "dipoles": 2048, "rhs_per_step": 2, "tol": C0["tol"],
+                   "grid": [16, 16, 8], "dipoles": 2048, "rhs_per_step": 2, "tol": SMALL16["tol"],
                    "why_not_the_gpu_workload": "the reference's BiCGSTAB does not reach 1e-8 on the 128x128x32 "
                                                "periodic workload (see the GPU arm's reference_algorithm_gpu)"},
         "samples_s_per_step": steps,
@@ -363,8 +363,8 @@ def run_reference(args):
                          "sample": f"full solves at 16x16x8, both polarisations, {len(steps)} timed steps after "
                                    f"{args.warmup} warm-up; oracle port (scipy.fft, {cores} workers)"},
         "operator_apply_s": {
-            "c1_64x64x16": {"median": statistics.median(s1), "samples": s1},
-            "c2_128x128x32": {"median": statistics.median(s2), "samples": s2},
+            "grid_64x64x16": {"median": statistics.median(s1), "samples": s1},
+            "grid_128x128x32": {"median": statistics.median(s2), "samples": s2},
             "note": "complex128 A.x + (1/alpha) x of the oracle port on the full grid (reference padding 2n-1)"},
         "e2e": {"value": sps, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -658,14 +658,14 @@ def summary(ts, infos):
             "gmres_steps": [i["iterations"] for i in infos], "refinements": [i["refinements"] for i in infos]}
 
 
-def run_c0_gpu(sici):
-    """configs[0] (the reference arm's workload) on the GPU: the reference's
+def run_isolated16_gpu(sici):
+    """The 16x16x8 isolated workload (the reference arm's) on the GPU: the reference's
     algorithm (unscaled complex128 BiCGSTAB from zero to a 1e-8 recursive
     residual) and the mixed-precision refinement, both polarisations."""
     rho = c0_design()
     out = {}
     for name, prec, solver in (("reference_algorithm", "complex128", "none"), ("mixed", "mixed", "jacobi")):
-        pair = PolPair(C0, sici, rho, precision="mixed")
+        pair = PolPair(SMALL16, sici, rho, precision="mixed")
         for m in pair.models:
             m.setPreconditioner(solver)
         pair.timed(prec, 2, 100000)
@@ -685,8 +685,8 @@ def run_isolated(sici, steps=2):
     return dict(summary(ts, infos), workload="128x128x32 isolated, mixed BiCGSTAB refinement")
 
 
-def run_periodic_c1(sici):
-    """64x64x16, periodic 64d, |m|,|n| <= 50, rho ~ U[0,1] per
+def run_periodic64(sici):
+    """The 64x64x16 workload: periodic 64d, |m|,|n| <= 50, rho ~ U[0,1] per
     dipole, complex128 throughout: the operator, a complex128 solve to 1e-8
     with the periodic solver, and the lattice sums."""
     from dda_model import DDAModel
@@ -709,7 +709,7 @@ def run_periodic_c1(sici):
 
 
 def run_gradient(sici):
-    """configs[4]'s differentiation step: 96x96x24 dipoles, periodic 96d,
+    """The differentiation step: 96x96x24 dipoles, periodic 96d,
     |m|,|n| <= 50, raw rho ~ U[0,1] -> radius-2 cone filter -> tanh (beta 8,
     eta 0.5) -> densities, objective mean |E|^2 over an 8x8x1 patch 3 cells
     above the top face; forward solve + adjoint gradient through
@@ -893,8 +893,8 @@ def main():
 
     extra = {}
     if not args.small:
-        for name, fn in (("isolated_c2", lambda: run_isolated(sici)), ("c0_gpu", lambda: run_c0_gpu(sici)),
-                         ("periodic_c1", lambda: run_periodic_c1(sici)), ("gradient_c4", lambda: run_gradient(sici)),
+        for name, fn in (("isolated_128x128x32", lambda: run_isolated(sici)), ("isolated_16x16x8_gpu", lambda: run_isolated16_gpu(sici)),
+                         ("periodic_64x64x16", lambda: run_periodic64(sici)), ("gradient_96x96x24", lambda: run_gradient(sici)),
                          ("reference_cufft_restatement", lambda: run_cufft_restatement(dict(w, M=0), sici))):
             extra[name] = fn()
             log(f"{name}: {json.dumps(extra[name])[:400]}")
@@ -966,7 +966,7 @@ def main():
             "clocks": clk.summary(),
             "gpu_launches": int(launches),
             "setup_s": setup_s,
-            "lattice_c2": lattice_record(m, w, lat_cpu),
+            "lattice_128x128x32": lattice_record(m, w, lat_cpu),
             **extra,
             "serving": serving,
         }

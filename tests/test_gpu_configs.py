@@ -1,4 +1,4 @@
-"""Full-size checks of the differentiation workload (configs[4]): 96x96x24
+"""Full-size checks of the differentiation workload: 96x96x24
 dipoles (221,184), periodic with period 96 d in x and y and the lattice sums
 over |m|,|n| <= 50, raw design rho ~ U[0, 1] -> radius-2 cone filter -> tanh
 projection (beta 8, eta 0.5), objective mean |E|^2 over an 8x8x1 patch 3

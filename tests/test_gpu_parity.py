@@ -42,7 +42,7 @@ def _rand(n, seed):
 
 
 @pytest.mark.parametrize("shape,periodic,method", [
-    ((16, 16, 8), 0, "FCD"),     # configs[0] grid, non-periodic
+    ((16, 16, 8), 0, "FCD"),     # the 16x16x8 benchmark grid, non-periodic
     ((8, 6, 4), 3, "FCD"),
     ((8, 6, 4), 3, "LDR"),
     ((5, 7, 3), 2, "FCD"),       # odd sizes: padded lengths 12/16/6 (radix 3)
