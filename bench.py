@@ -268,7 +268,7 @@ def dist_setup():
 SMALL16 = dict(WORKLOAD, nx=16, ny=16, nz=8, period=16, M=0, seed=7)
 
 
-def c0_design():
+def small16_design():
     return np.random.default_rng(SMALL16["seed"]).random(SMALL16["nx"] * SMALL16["ny"] * SMALL16["nz"])
 
 
@@ -322,7 +322,7 @@ def run_reference(args):
     world, rank, local = dist_setup()
     if rank != 0:
         return 0
-    rho0 = c0_design()
+    rho0 = small16_design()
     ports = [CpuPort(SMALL16, rho0, pol) for pol in (0, 1)]
     cores = ports[0].cores
     steps, infos = [], []
@@ -662,7 +662,7 @@ def run_isolated16_gpu(sici):
     """The 16x16x8 isolated workload (the reference arm's) on the GPU: the reference's
     algorithm (unscaled complex128 BiCGSTAB from zero to a 1e-8 recursive
     residual) and the mixed-precision refinement, both polarisations."""
-    rho = c0_design()
+    rho = small16_design()
     out = {}
     for name, prec, solver in (("reference_algorithm", "complex128", "none"), ("mixed", "mixed", "jacobi")):
         pair = PolPair(SMALL16, sici, rho, precision="mixed")
